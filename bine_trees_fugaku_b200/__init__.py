@@ -1,0 +1,299 @@
+"""B200-native engine for the Bine-tree collectives over virtual ranks.
+
+Python mirror of the engine's C ABI (include/bine_b200.h), loaded with ctypes
+from the in-tree library lib/libbine_b200.so.  A ``Comm`` holds P virtual
+ranks on one GPU; its methods keep the argument lists of the reference's MPI
+entry points (lib/libbine.cc): ``allreduce(sendbuf, recvbuf, count, datatype,
+op)``, ``bcast(buffer, count, datatype, root)`` and so on, where every
+buffer is a rank-major device array -- a CUDA torch tensor of shape
+(P, row) or a raw device pointer.
+
+There is no fallback: if the library is missing, importing the engine
+raises, and every call runs the CUDA kernels.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .build import LIB_PATH
+
+INT32, INT64, FLOAT, DOUBLE, CHAR = 0, 1, 2, 3, 4
+SUM = 0
+SUCCESS, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_INTERNAL = range(7)
+ENGINE_FUSED, ENGINE_STEPS = 0, 1
+ORDER_REFERENCE, ORDER_FAST = 0, 1
+FAMILY = {"BINE": 1, "RECDOUB": 2}
+DISTANCE = {None: -1, "INCREASING": 0, "DECREASING": 1}
+
+COLLS = ["allreduce", "reduce_scatter", "allgather", "bcast", "reduce", "alltoall", "scatter", "gather"]
+COLL_ID = {c: i for i, c in enumerate(COLLS)}
+# Variant names are the reference's LIBBINE_<COLL>_ALGO values.
+VARIANTS = {
+    "allreduce": {"L": 0, "B": 1, "B_CONT": 3, "B_COALESCE": 4},
+    "reduce_scatter": {"VEC_HALVING_CONT_PERMUTE": 0},
+    "allgather": {"VEC_DOUBLING_CONT_PERMUTE": 0, "VEC_DOUBLING_CONT_SEND": 1, "VEC_DOUBLING_BLOCKS": 2},
+    "bcast": {"BINOMIAL_TREE": 0, "SCATTER_ALLGATHER": 2},
+    "reduce": {"BINOMIAL_TREE": 0, "REDUCE_SCATTER_GATHER": 1},
+    "alltoall": {"LOG": 0},
+    "scatter": {"BINOMIAL_TREE_CONT_PERMUTE": 0},
+    "gather": {"BINOMIAL_TREE_CONT_PERMUTE": 0},
+}
+DTYPE_SIZE = {INT32: 4, INT64: 8, FLOAT: 4, DOUBLE: 8, CHAR: 1}
+NP_DTYPE = {INT32: np.int32, INT64: np.int64, FLOAT: np.float32, DOUBLE: np.float64, CHAR: np.int8}
+
+
+class BineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"bine error {code}: {msg}")
+        self.code = code
+
+
+class Unsupported(BineError):
+    """The selected reference algorithm cannot run this case."""
+
+
+class Timeout(BineError):
+    """A bounded device-side wait expired."""
+
+
+_lib = None
+
+
+def lib():
+    """Loads lib/libbine_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"the engine library is not built: {LIB_PATH} "
+                          "(run `python -m bine_trees_fugaku_b200.build`)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, ci, sz, i64p = ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64)
+    L.bine_last_error_string.restype = ctypes.c_char_p
+    sig = {
+        "bine_comm_create": [i, i, ctypes.POINTER(ci), ctypes.POINTER(vp)],
+        "bine_comm_destroy": [vp],
+        "bine_comm_set_stream": [vp, vp],
+        "bine_comm_set_layout": [vp, sz, sz],
+        "bine_comm_set_ports": [vp, i],
+        "bine_comm_set_algo": [vp, i, i, i, i],
+        "bine_comm_set_engine": [vp, i],
+        "bine_comm_set_float_order": [vp, i],
+        "bine_comm_set_step_timeout": [vp, ctypes.c_uint],
+        "bine_debug_set_barrier_extra": [vp, ctypes.c_uint],
+        "bine_comm_synchronize": [vp],
+        "bine_allreduce": [vp, vp, i, i, i, vp],
+        "bine_reduce_scatter": [vp, vp, ctypes.POINTER(ci), i, i, vp],
+        "bine_allgather": [vp, i, i, vp, i, i, vp],
+        "bine_bcast": [vp, i, i, i, vp],
+        "bine_alltoall": [vp, i, i, vp, i, i, vp],
+        "bine_scatter": [vp, i, i, vp, i, i, i, vp],
+        "bine_gather": [vp, i, i, vp, i, i, i, vp],
+        "bine_reduce": [vp, vp, i, i, i, i, vp],
+        "bine_plan_stats": [vp, i, ctypes.c_long, i, i64p],
+        "bine_plan_moves": [vp, i, ctypes.c_long, i, i64p, i64p, sz, ctypes.POINTER(sz)],
+        "bine_plan_messages": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz)],
+        "bine_plan_trees": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz)],
+        "bine_link_bytes_host": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(ctypes.c_uint64), sz],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def last_error():
+    return lib().bine_last_error_string().decode()
+
+
+def check(rc):
+    if rc == SUCCESS:
+        return
+    msg = last_error()
+    if rc == ERR_UNSUPPORTED:
+        raise Unsupported(rc, msg)
+    if rc == ERR_TIMEOUT:
+        raise Timeout(rc, msg)
+    raise BineError(rc, msg)
+
+
+def _ptr(buf):
+    """Device pointer of a CUDA tensor or an integer address."""
+    if buf is None:
+        return None
+    if isinstance(buf, int):
+        return buf
+    if hasattr(buf, "data_ptr"):
+        if not buf.is_cuda:
+            raise ValueError("buffers must be CUDA tensors (device memory)")
+        return buf.data_ptr()
+    raise TypeError(f"unsupported buffer type {type(buf)}")
+
+
+def dtype_of_tensor(t):
+    import torch
+    return {torch.int32: INT32, torch.int64: INT64, torch.float32: FLOAT, torch.float64: DOUBLE,
+            torch.int8: CHAR}[t.dtype]
+
+
+class Comm:
+    """P virtual ranks on the current CUDA device (a torus of `dims`)."""
+
+    def __init__(self, nranks, dims=None):
+        dims = list(dims or [])
+        arr = (ctypes.c_int * max(1, len(dims)))(*dims) if dims else None
+        h = ctypes.c_void_p()
+        check(lib().bine_comm_create(nranks, len(dims), arr, ctypes.byref(h)))
+        self._h = h
+        self.nranks = nranks
+        self.dims = dims or [nranks]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bine_comm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --------------------------------------------------------- settings
+    def set_stream(self, stream):
+        """Orders calls on a torch.cuda.Stream (or a raw cudaStream_t)."""
+        h = stream if isinstance(stream, int) else (stream.cuda_stream if stream is not None else 0)
+        check(lib().bine_comm_set_stream(self._h, h))
+
+    def set_layout(self, send_stride=0, recv_stride=0):
+        check(lib().bine_comm_set_layout(self._h, send_stride, recv_stride))
+
+    def set_ports(self, ports):
+        check(lib().bine_comm_set_ports(self._h, ports))
+
+    def set_algo(self, coll, variant, family="BINE", distance=None):
+        check(lib().bine_comm_set_algo(self._h, COLL_ID[coll], VARIANTS[coll][variant], FAMILY[family],
+                                       DISTANCE[distance]))
+
+    def set_engine(self, engine):
+        check(lib().bine_comm_set_engine(self._h, {"fused": ENGINE_FUSED, "steps": ENGINE_STEPS}.get(engine, engine)))
+
+    def set_float_order(self, order):
+        check(lib().bine_comm_set_float_order(self._h, {"reference": ORDER_REFERENCE, "fast": ORDER_FAST}.get(order, order)))
+
+    def set_step_timeout(self, ms):
+        check(lib().bine_comm_set_step_timeout(self._h, ms))
+
+    def debug_set_barrier_extra(self, extra):
+        check(lib().bine_debug_set_barrier_extra(self._h, extra))
+
+    def synchronize(self):
+        check(lib().bine_comm_synchronize(self._h))
+
+    # ------------------------------------------------------ collectives
+    def allreduce(self, sendbuf, recvbuf, count, datatype, op=SUM):
+        check(lib().bine_allreduce(_ptr(sendbuf), _ptr(recvbuf), count, datatype, op, self._h))
+
+    def reduce_scatter(self, sendbuf, recvbuf, recvcounts, datatype, op=SUM):
+        rc = (ctypes.c_int * self.nranks)(*recvcounts)
+        check(lib().bine_reduce_scatter(_ptr(sendbuf), _ptr(recvbuf), rc, datatype, op, self._h))
+
+    def allgather(self, sendbuf, sendcount, sendtype, recvbuf, recvcount, recvtype):
+        check(lib().bine_allgather(_ptr(sendbuf), sendcount, sendtype, _ptr(recvbuf), recvcount, recvtype, self._h))
+
+    def bcast(self, buffer, count, datatype, root):
+        check(lib().bine_bcast(_ptr(buffer), count, datatype, root, self._h))
+
+    def alltoall(self, sendbuf, sendcount, sendtype, recvbuf, recvcount, recvtype):
+        check(lib().bine_alltoall(_ptr(sendbuf), sendcount, sendtype, _ptr(recvbuf), recvcount, recvtype, self._h))
+
+    def scatter(self, sendbuf, sendcount, sendtype, recvbuf, recvcount, recvtype, root):
+        check(lib().bine_scatter(_ptr(sendbuf), sendcount, sendtype, _ptr(recvbuf), recvcount, recvtype, root,
+                                 self._h))
+
+    def gather(self, sendbuf, sendcount, sendtype, recvbuf, recvcount, recvtype, root):
+        check(lib().bine_gather(_ptr(sendbuf), sendcount, sendtype, _ptr(recvbuf), recvcount, recvtype, root,
+                                self._h))
+
+    def reduce(self, sendbuf, recvbuf, count, datatype, op=SUM, root=0):
+        check(lib().bine_reduce(_ptr(sendbuf), _ptr(recvbuf), count, datatype, op, root, self._h))
+
+    def run(self, coll, sendbuf, recvbuf, count, datatype, root=0):
+        """Dispatches by name with the reference's `count` meaning."""
+        if coll == "allreduce":
+            return self.allreduce(sendbuf, recvbuf, count, datatype)
+        if coll == "reduce_scatter":
+            return self.reduce_scatter(sendbuf, recvbuf, [count] * self.nranks, datatype)
+        if coll == "allgather":
+            return self.allgather(sendbuf, count, datatype, recvbuf, count, datatype)
+        if coll == "bcast":
+            return self.bcast(recvbuf, count, datatype, root)
+        if coll == "reduce":
+            return self.reduce(sendbuf, recvbuf, count, datatype, SUM, root)
+        if coll == "alltoall":
+            return self.alltoall(sendbuf, count, datatype, recvbuf, count, datatype)
+        if coll == "scatter":
+            return self.scatter(sendbuf, count, datatype, recvbuf, count, datatype, root)
+        if coll == "gather":
+            return self.gather(sendbuf, count, datatype, recvbuf, count, datatype, root)
+        raise ValueError(coll)
+
+    # -------------------------------------------- host schedule queries
+    def plan_stats(self, coll, count, root=0):
+        out = (ctypes.c_int64 * 5)()
+        check(lib().bine_plan_stats(self._h, COLL_ID[coll], count, root, out))
+        return dict(zip(["levels", "moves", "messages", "tmp_elems", "traffic_elems"], list(out)))
+
+    def plan_moves(self, coll, count, root=0):
+        n = ctypes.c_size_t(0)
+        check(lib().bine_plan_moves(self._h, COLL_ID[coll], count, root, None, None, 0, ctypes.byref(n)))
+        mv = np.zeros((max(1, n.value), 10), np.int64)
+        sz = np.zeros(max(1, n.value), np.int64)
+        check(lib().bine_plan_moves(self._h, COLL_ID[coll], count, root,
+                                    mv.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                    sz.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n.value, ctypes.byref(n)))
+        return mv[: n.value], sz[: n.value] // 2, sz[: n.value] % 2
+
+    def plan_messages(self, coll, count, root=0):
+        n = ctypes.c_size_t(0)
+        check(lib().bine_plan_messages(self._h, COLL_ID[coll], count, root, None, 0, ctypes.byref(n)))
+        m = np.zeros((max(1, n.value), 4), np.int64)
+        check(lib().bine_plan_messages(self._h, COLL_ID[coll], count, root,
+                                       m.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n.value, ctypes.byref(n)))
+        return m[: n.value]
+
+    def plan_trees(self, coll, count, root=0):
+        npg, nsg = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        check(lib().bine_plan_trees(self._h, COLL_ID[coll], count, root, None, 0, ctypes.byref(npg), None, 0,
+                                    ctypes.byref(nsg)))
+        prog = np.zeros((max(1, npg.value), 3), np.int64)
+        segs = np.zeros((max(1, nsg.value), 6), np.int64)
+        p64 = ctypes.POINTER(ctypes.c_int64)
+        check(lib().bine_plan_trees(self._h, COLL_ID[coll], count, root, prog.ctypes.data_as(p64), npg.value,
+                                    ctypes.byref(npg), segs.ctypes.data_as(p64), nsg.value, ctypes.byref(nsg)))
+        return prog[: npg.value], segs[: nsg.value]
+
+    def link_bytes_host(self, coll, count, datatype, root=0):
+        n = self.nranks * len(self.dims) * 2
+        out = np.zeros(n, np.uint64)
+        check(lib().bine_link_bytes_host(self._h, COLL_ID[coll], count, datatype, root,
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), n))
+        return out
+
+
+def row_counts(coll, count, P):
+    """Per-rank (send, receive) element counts for the reference's `count`."""
+    if coll in ("allreduce", "reduce"):
+        return count, count
+    if coll == "bcast":
+        return 0, count
+    if coll in ("reduce_scatter", "scatter"):
+        return count * P, count
+    if coll in ("allgather", "gather"):
+        return count, count * P
+    if coll == "alltoall":
+        return count * P, count * P
+    raise ValueError(coll)

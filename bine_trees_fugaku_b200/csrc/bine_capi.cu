@@ -1,0 +1,787 @@
+// C ABI of the B200 Bine engine (include/bine_b200.h): communicator state,
+// plan caches, dispatch of the eight collectives to the fused kernels or the
+// step engine, and the host-side schedule queries.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/bine_b200.h"
+#include "bine_kernels.cuh"
+#include "bine_plan.h"
+
+using namespace bine;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                               \
+    do {                                                                                             \
+        cudaError_t e_ = (expr);                                                                     \
+        if (e_ != cudaSuccess) {                                                                     \
+            return fail(e_ == cudaErrorMemoryAllocation ? BINE_ERR_NOMEM : BINE_ERR_CUDA,            \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                         \
+        }                                                                                            \
+    } while (0)
+
+int dtype_size(int dt) {
+    switch (dt) {
+    case BINE_INT32: return 4;
+    case BINE_INT64: return 8;
+    case BINE_FLOAT: return 4;
+    case BINE_DOUBLE: return 8;
+    case BINE_CHAR: return 1;
+    default: return -1;
+    }
+}
+
+struct CollCfg {
+    int variant, family, distance;
+};
+
+// Default variant and distance of every collective: lib/libbine.cc:56-72.
+const CollCfg kDefaults[kNumColls] = {
+    {kArB, kFamilyBine, kIncreasing},           {kRsContPermute, kFamilyBine, kIncreasing},
+    {kAgContPermute, kFamilyBine, kDecreasing}, {kBcTree, kFamilyBine, kDecreasing},
+    {kRdTree, kFamilyBine, kIncreasing},        {kA2aLog, kFamilyBine, kIncreasing},
+    {kScTree, kFamilyBine, kIncreasing},        {kGaTree, kFamilyBine, kDecreasing}};
+
+// Device copy of one schedule for the step engine.
+struct DevSteps {
+    dev::StepMove* moves = nullptr;
+    dev::StepChunk* chunks = nullptr;
+    int* level_begin = nullptr;
+    int nlevels = 0;
+    int max_chunks_per_level = 0;
+    int64_t tmp_elems = 0;
+    ~DevSteps() {
+        cudaFree(moves);
+        cudaFree(chunks);
+        cudaFree(level_begin);
+    }
+};
+
+// Device copy of the exact reduction trees of one call.
+struct DevTrees {
+    dev::TreeSeg* segs = nullptr;
+    dev::TreeEntry* prog = nullptr;
+    dev::TreeTile* tiles = nullptr;
+    int ntiles = 0;
+    int max_prog_len = 0;
+    bool vec_ok = false;  // every offset and shift is a multiple of 16 bytes
+    ~DevTrees() {
+        cudaFree(segs);
+        cudaFree(prog);
+        cudaFree(tiles);
+    }
+};
+
+struct PlanKeyEs {
+    PlanKey k;
+    int es;
+    bool operator==(const PlanKeyEs& o) const { return k == o.k && es == o.es; }
+};
+struct PlanKeyEsHash {
+    size_t operator()(const PlanKeyEs& x) const { return PlanKeyHash()(x.k) * 31 + (size_t)x.es; }
+};
+
+}  // namespace
+
+struct bine_comm_s {
+    int P = 0;
+    std::unique_ptr<Planner> planner;
+    cudaStream_t stream = nullptr;
+    size_t send_stride = 0, recv_stride = 0;
+    int ports = 1;
+    int engine = BINE_ENGINE_FUSED;
+    int order = BINE_ORDER_REFERENCE;
+    CollCfg cfg[kNumColls];
+    std::mutex mu;
+    std::unordered_map<PlanKey, std::shared_ptr<Schedule>, PlanKeyHash> schedules;
+    std::unordered_map<PlanKeyEs, std::shared_ptr<DevSteps>, PlanKeyEsHash> dev_steps;
+    std::unordered_map<PlanKeyEs, std::shared_ptr<DevTrees>, PlanKeyEsHash> dev_trees;
+    // Device state, created on first use.
+    int device = -1;
+    int num_sms = 0;
+    char* work = nullptr;
+    size_t work_bytes = 0;
+    unsigned* barrier = nullptr;  // [0] arrivals, [1] generation
+    int* status = nullptr;
+    unsigned long long step_timeout_ns = 5ull * 1000 * 1000 * 1000;
+    unsigned barrier_extra = 0;
+    ~bine_comm_s() {
+        cudaFree(work);
+        cudaFree(barrier);
+        cudaFree(status);
+    }
+};
+
+namespace {
+
+PlanKey make_key(bine_comm_t c, int coll, long count, int root) {
+    PlanKey k;
+    k.coll = coll;
+    k.variant = c->cfg[coll].variant;
+    k.family = c->cfg[coll].family;
+    k.distance = c->cfg[coll].distance;
+    k.ports = c->ports;
+    k.root = root;
+    k.count = count;
+    return k;
+}
+
+int get_schedule(bine_comm_t c, const PlanKey& k, std::shared_ptr<Schedule>* out) {
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto it = c->schedules.find(k);
+    if (it != c->schedules.end()) {
+        *out = it->second;
+        return BINE_SUCCESS;
+    }
+    auto s = std::make_shared<Schedule>();
+    std::string err;
+    if (!c->planner->build(k, s.get(), &err)) return fail(BINE_ERR_UNSUPPORTED, err);
+    c->schedules.emplace(k, s);
+    *out = s;
+    return BINE_SUCCESS;
+}
+
+int ensure_device(bine_comm_t c) {
+    if (c->device >= 0) return BINE_SUCCESS;
+    int dev;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+    CUDA_TRY(cudaMalloc(&c->barrier, 2 * sizeof(unsigned)));
+    CUDA_TRY(cudaMalloc(&c->status, sizeof(int)));
+    CUDA_TRY(cudaMemset(c->barrier, 0, 2 * sizeof(unsigned)));
+    CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
+    c->device = dev;
+    return BINE_SUCCESS;
+}
+
+int ensure_work(bine_comm_t c, size_t bytes) {
+    if (bytes <= c->work_bytes) return BINE_SUCCESS;
+    // Stream-ordered reuse: wait for pending work before replacing the area.
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    cudaFree(c->work);
+    c->work = nullptr;
+    c->work_bytes = 0;
+    CUDA_TRY(cudaMalloc(&c->work, bytes));
+    c->work_bytes = bytes;
+    return BINE_SUCCESS;
+}
+
+template <typename T>
+void fill(T** dptr, const std::vector<T>& v, cudaError_t* err) {
+    *err = cudaMalloc(dptr, std::max<size_t>(1, v.size()) * sizeof(T));
+    if (*err == cudaSuccess && !v.empty()) *err = cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+int get_dev_steps(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSteps>* out) {
+    std::shared_ptr<Schedule> s;
+    int rc = get_schedule(c, k, &s);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    PlanKeyEs key{k, es};
+    auto it = c->dev_steps.find(key);
+    if (it != c->dev_steps.end()) {
+        *out = it->second;
+        return BINE_SUCCESS;
+    }
+    auto d = std::make_shared<DevSteps>();
+    std::vector<dev::StepMove> moves;
+    std::vector<dev::StepChunk> chunks;
+    std::vector<int> lb;
+    const int64_t chunk_elems = std::max<int64_t>(16, (32 * 1024) / es);
+    for (const auto& lvl : s->levels) {
+        lb.push_back((int)chunks.size());
+        for (const Move& m : lvl) {
+            dev::StepMove dm;
+            dm.dst_off = m.dst.off;
+            dm.a_off = m.a.off;
+            dm.b_off = m.b.off;
+            dm.dst_rank = m.dst.rank;
+            dm.a_rank = m.a.rank;
+            dm.b_rank = m.b.rank;
+            dm.dst_buf = m.dst.buf;
+            dm.a_buf = m.a.buf;
+            dm.b_buf = m.b.buf;
+            dm.add = m.add;
+            const int mi = (int)moves.size();
+            moves.push_back(dm);
+            for (int64_t st = 0; st < m.n; st += chunk_elems)
+                chunks.push_back(dev::StepChunk{mi, 0, st, std::min(chunk_elems, m.n - st)});
+        }
+        int nlvl = (int)chunks.size() - lb.back();
+        d->max_chunks_per_level = std::max(d->max_chunks_per_level, nlvl);
+    }
+    lb.push_back((int)chunks.size());
+    d->nlevels = (int)s->levels.size();
+    d->tmp_elems = s->tmp_elems;
+    cudaError_t e1, e2, e3;
+    fill(&d->moves, moves, &e1);
+    fill(&d->chunks, chunks, &e2);
+    fill(&d->level_begin, lb, &e3);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        return fail(BINE_ERR_CUDA, "uploading the schedule failed");
+    c->dev_steps.emplace(key, d);
+    *out = d;
+    return BINE_SUCCESS;
+}
+
+int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTrees>* out) {
+    std::shared_ptr<Schedule> s;
+    int rc = get_schedule(c, k, &s);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    PlanKeyEs key{k, es};
+    auto it = c->dev_trees.find(key);
+    if (it != c->dev_trees.end()) {
+        *out = it->second;
+        return BINE_SUCCESS;
+    }
+    TreePlan tp;
+    std::string err;
+    if (!c->planner->trees(k, *s, &tp, &err)) return fail(BINE_ERR_INTERNAL, err);
+    if (tp.max_depth > dev::kMaxTreeDepth) return fail(BINE_ERR_UNSUPPORTED, "reduction tree deeper than supported");
+    auto d = std::make_shared<DevTrees>();
+    std::vector<dev::TreeSeg> segs;
+    std::vector<dev::TreeEntry> prog;
+    std::vector<dev::TreeTile> tiles;
+    bool vec = true;
+    for (const ProgEntry& e : tp.prog) {
+        prog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
+        if ((e.shift * es) % 16) vec = false;
+    }
+    for (const OutSegment& sg : tp.segs) {
+        segs.push_back(dev::TreeSeg{sg.off, sg.n, sg.rank, sg.prog_begin, sg.prog_len, sg.depth});
+        d->max_prog_len = std::max(d->max_prog_len, sg.prog_len);
+        if ((sg.off * es) % 16 || (sg.n * es) % 16) vec = false;
+    }
+    const int64_t tile = vec ? (int64_t)dev::kThreads * (16 / es) : (int64_t)dev::kThreads * 4;
+    for (size_t i = 0; i < tp.segs.size(); i++)
+        for (int64_t st = 0; st < tp.segs[i].n; st += tile)
+            tiles.push_back(dev::TreeTile{(int32_t)i, 0, st, std::min(tile, tp.segs[i].n - st)});
+    d->ntiles = (int)tiles.size();
+    d->vec_ok = vec;
+    cudaError_t e1, e2, e3;
+    fill(&d->segs, segs, &e1);
+    fill(&d->prog, prog, &e2);
+    fill(&d->tiles, tiles, &e3);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        return fail(BINE_ERR_CUDA, "uploading the reduction trees failed");
+    c->dev_trees.emplace(key, d);
+    *out = d;
+    return BINE_SUCCESS;
+}
+
+unsigned grid_for(const bine_comm_t c, long long work_items) {
+    long long blocks = (work_items + dev::kThreads - 1) / dev::kThreads;
+    long long cap = (long long)std::max(1, c->num_sms) * 16;
+    return (unsigned)std::max(1LL, std::min(blocks, cap));
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+// ---------------------------------------------------------- fused kernels
+template <typename T>
+int launch_sum(bine_comm_t c, int mode, const char* in, long long ist, char* out, long long ost, long long elems,
+               long long blk, int root) {
+    const int P = c->P;
+    const long long es = sizeof(T);
+    const bool vec = aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0 &&
+                     (mode != dev::kSumReduceScatter || (blk * es) % 16 == 0);
+    long long done = 0;
+    if (vec) {
+        const long long ncol = elems * es / 16;
+        if (ncol > 0) {
+            unsigned g = grid_for(c, ncol);
+            const long long blk_vec = mode == dev::kSumReduceScatter ? blk * es / 16 : 0;
+            if (mode == dev::kSumAllreduce)
+                dev::k_sum_vec<T, dev::kSumAllreduce><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol, blk_vec, root);
+            else if (mode == dev::kSumReduceScatter)
+                dev::k_sum_vec<T, dev::kSumReduceScatter><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol, blk_vec, root);
+            else
+                dev::k_sum_vec<T, dev::kSumReduce><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol, blk_vec, root);
+            done = ncol * 16 / es;
+        }
+    }
+    const long long rest = elems - done;
+    if (rest > 0) {
+        unsigned g = grid_for(c, rest);
+        if (mode == dev::kSumAllreduce)
+            dev::k_sum_scalar<T, dev::kSumAllreduce><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, done, rest, blk, root);
+        else if (mode == dev::kSumReduceScatter)
+            dev::k_sum_scalar<T, dev::kSumReduceScatter><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, done, rest, blk, root);
+        else
+            dev::k_sum_scalar<T, dev::kSumReduce><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, done, rest, blk, root);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
+int launch_sum_dt(bine_comm_t c, int dt, int mode, const char* in, long long ist, char* out, long long ost,
+                  long long elems, long long blk, int root) {
+    switch (dt) {
+    case BINE_INT32: return launch_sum<int32_t>(c, mode, in, ist, out, ost, elems, blk, root);
+    case BINE_INT64: return launch_sum<int64_t>(c, mode, in, ist, out, ost, elems, blk, root);
+    case BINE_FLOAT: return launch_sum<float>(c, mode, in, ist, out, ost, elems, blk, root);
+    case BINE_DOUBLE: return launch_sum<double>(c, mode, in, ist, out, ost, elems, blk, root);
+    case BINE_CHAR: return launch_sum<int8_t>(c, mode, in, ist, out, ost, elems, blk, root);
+    }
+    return fail(BINE_ERR_ARG, "bad datatype");
+}
+
+template <typename T>
+int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost) {
+    if (d.ntiles == 0) return BINE_SUCCESS;
+    const size_t smem = (size_t)d.max_prog_len * sizeof(dev::TreeEntry);
+    const bool vec = d.vec_ok && aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0;
+    auto kern = vec ? dev::k_tree_vec<T> : dev::k_tree_scalar<T>;
+    if (smem > 227 * 1024) return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
+    if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    unsigned g = (unsigned)std::min<long long>(d.ntiles, (long long)std::max(1, c->num_sms) * 8);
+    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.segs, d.prog, d.tiles, d.ntiles);
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
+int launch_copy(bine_comm_t c, int mode, const char* in, long long ist, char* out, long long ost, long long unit,
+                int root, int es) {
+    dev::CopyArgs a{in, ist, out, ost, c->P, root, unit};
+    long long pairs = mode == dev::kCopyAlltoall ? (long long)c->P * c->P : (mode == dev::kCopyBcast ? 1 : c->P);
+    if (unit == 0) return BINE_SUCCESS;
+    const bool vec = aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0 && unit % 16 == 0;
+    if (vec) {
+        unsigned g = grid_for(c, pairs * (unit / 16));
+        switch (mode) {
+        case dev::kCopyAllgather: dev::k_copy_vec<dev::kCopyAllgather><<<g, dev::kThreads, 0, c->stream>>>(a); break;
+        case dev::kCopyBcast: dev::k_copy_vec<dev::kCopyBcast><<<g, dev::kThreads, 0, c->stream>>>(a); break;
+        case dev::kCopyAlltoall: dev::k_copy_vec<dev::kCopyAlltoall><<<g, dev::kThreads, 0, c->stream>>>(a); break;
+        case dev::kCopyScatter: dev::k_copy_vec<dev::kCopyScatter><<<g, dev::kThreads, 0, c->stream>>>(a); break;
+        case dev::kCopyGather: dev::k_copy_vec<dev::kCopyGather><<<g, dev::kThreads, 0, c->stream>>>(a); break;
+        }
+    } else {
+        unsigned g = grid_for(c, pairs * (unit / es));
+#define BINE_COPY_SCALAR(U)                                                                                          \
+    switch (mode) {                                                                                                  \
+    case dev::kCopyAllgather: dev::k_copy_scalar<dev::kCopyAllgather, U><<<g, dev::kThreads, 0, c->stream>>>(a); break; \
+    case dev::kCopyBcast: dev::k_copy_scalar<dev::kCopyBcast, U><<<g, dev::kThreads, 0, c->stream>>>(a); break;         \
+    case dev::kCopyAlltoall: dev::k_copy_scalar<dev::kCopyAlltoall, U><<<g, dev::kThreads, 0, c->stream>>>(a); break;   \
+    case dev::kCopyScatter: dev::k_copy_scalar<dev::kCopyScatter, U><<<g, dev::kThreads, 0, c->stream>>>(a); break;     \
+    case dev::kCopyGather: dev::k_copy_scalar<dev::kCopyGather, U><<<g, dev::kThreads, 0, c->stream>>>(a); break;       \
+    }
+        if (es == 8 && ((uintptr_t)in | (uintptr_t)out | ist | ost | unit) % 8 == 0) {
+            BINE_COPY_SCALAR(uint64_t)
+        } else if (es >= 4 && ((uintptr_t)in | (uintptr_t)out | ist | ost | unit) % 4 == 0) {
+            BINE_COPY_SCALAR(uint32_t)
+        } else {
+            BINE_COPY_SCALAR(uint8_t)
+        }
+#undef BINE_COPY_SCALAR
+    }
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
+// ------------------------------------------------------------ step engine
+template <typename T>
+int launch_steps(bine_comm_t c, const DevSteps& d, const char* send, long long ist, char* recv, long long ost) {
+    if (d.nlevels == 0) return BINE_SUCCESS;
+    const size_t es = sizeof(T);
+    const size_t tmp_stride = ((size_t)d.tmp_elems * es + 255) / 256 * 256;
+    int rc = ensure_work(c, std::max<size_t>(tmp_stride * c->P, 256));
+    if (rc) return rc;
+    dev::StepBufs B;
+    B.base[kBufSend] = const_cast<char*>(send);
+    B.base[kBufRecv] = recv;
+    B.base[kBufTmp] = c->work;
+    B.stride[kBufSend] = ist;
+    B.stride[kBufRecv] = ost;
+    B.stride[kBufTmp] = (long long)tmp_stride;
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_steps<T>, dev::kThreads, 0));
+    int blocks = std::max(1, std::min(per_sm * c->num_sms, std::max(1, d.max_chunks_per_level)));
+    CUDA_TRY(cudaMemsetAsync(c->barrier, 0, 2 * sizeof(unsigned), c->stream));
+    const dev::StepMove* moves = d.moves;
+    const dev::StepChunk* chunks = d.chunks;
+    const int* lb = d.level_begin;
+    int nl = d.nlevels;
+    unsigned* bar = c->barrier;
+    int* status = c->status;
+    unsigned long long to = c->step_timeout_ns;
+    unsigned expected = (unsigned)blocks + c->barrier_extra;
+    void* args[] = {&B, &moves, &chunks, &lb, &nl, &bar, &status, &to, &expected};
+    CUDA_TRY(cudaLaunchCooperativeKernel((void*)dev::k_steps<T>, dim3(blocks), dim3(dev::kThreads), args, 0, c->stream));
+    return BINE_SUCCESS;
+}
+
+int launch_steps_dt(bine_comm_t c, int dt, const DevSteps& d, const char* send, long long ist, char* recv,
+                    long long ost) {
+    switch (dt) {
+    case BINE_INT32: return launch_steps<int32_t>(c, d, send, ist, recv, ost);
+    case BINE_INT64: return launch_steps<int64_t>(c, d, send, ist, recv, ost);
+    case BINE_FLOAT: return launch_steps<float>(c, d, send, ist, recv, ost);
+    case BINE_DOUBLE: return launch_steps<double>(c, d, send, ist, recv, ost);
+    case BINE_CHAR: return launch_steps<int8_t>(c, d, send, ist, recv, ost);
+    }
+    return fail(BINE_ERR_ARG, "bad datatype");
+}
+
+bool is_reduction(int coll) { return coll == kAllreduce || coll == kReduceScatter || coll == kReduce; }
+
+// Per-rank element counts of the send and receive rows.
+void row_elems(int coll, long long count, int P, long long* se, long long* re) {
+    switch (coll) {
+    case kAllreduce:
+    case kReduce: *se = count; *re = count; break;
+    case kBcast: *se = 0; *re = count; break;
+    case kReduceScatter:
+    case kScatter: *se = count * P; *re = count; break;
+    case kAllgather:
+    case kGather: *se = count; *re = count * P; break;
+    case kAlltoall: *se = count * P; *re = count * P; break;
+    default: *se = *re = 0;
+    }
+}
+
+int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, long long count, int dt, int root) {
+    if (!c) return fail(BINE_ERR_ARG, "null communicator");
+    const int es = dtype_size(dt);
+    if (es < 0) return fail(BINE_ERR_ARG, "invalid datatype");
+    if (count < 0) return fail(BINE_ERR_ARG, "negative count");
+    if (root < 0 || root >= c->P) return fail(BINE_ERR_ARG, "root out of range");
+    long long se, re;
+    row_elems(coll, count, c->P, &se, &re);
+    if ((se && !sendbuf) || (re && !recvbuf)) return fail(BINE_ERR_ARG, "null buffer");
+    const long long ist = c->send_stride ? (long long)c->send_stride : se * es;
+    const long long ost = c->recv_stride ? (long long)c->recv_stride : re * es;
+    if (ist < se * es || ost < re * es) return fail(BINE_ERR_ARG, "layout stride smaller than a rank row");
+    if (count == 0) return BINE_SUCCESS;
+    int rc = ensure_device(c);
+    if (rc) return rc;
+    const char* in = (const char*)sendbuf;
+    char* out = (char*)recvbuf;
+    PlanKey k = make_key(c, coll, count, root);
+
+    if (c->engine == BINE_ENGINE_STEPS) {
+        std::shared_ptr<DevSteps> d;
+        rc = get_dev_steps(c, k, es, &d);
+        if (rc) return rc;
+        return launch_steps_dt(c, dt, *d, in, ist, out, ost);
+    }
+
+    if (is_reduction(coll)) {
+        const bool exact = (dt == BINE_FLOAT || dt == BINE_DOUBLE) && c->order == BINE_ORDER_REFERENCE;
+        if (exact) {
+            std::shared_ptr<DevTrees> d;
+            rc = get_dev_trees(c, k, es, &d);
+            if (rc) return rc;
+            return dt == BINE_FLOAT ? launch_tree<float>(c, *d, in, ist, out, ost)
+                                    : launch_tree<double>(c, *d, in, ist, out, ost);
+        }
+        const int mode = coll == kAllreduce ? dev::kSumAllreduce
+                                            : (coll == kReduceScatter ? dev::kSumReduceScatter : dev::kSumReduce);
+        return launch_sum_dt(c, dt, mode, in, ist, out, ost, se, count, root);
+    }
+    switch (coll) {
+    case kAllgather: return launch_copy(c, dev::kCopyAllgather, in, ist, out, ost, count * es, root, es);
+    case kBcast: return launch_copy(c, dev::kCopyBcast, out, ost, out, ost, count * es, root, es);
+    case kAlltoall: return launch_copy(c, dev::kCopyAlltoall, in, ist, out, ost, count * es, root, es);
+    case kScatter: return launch_copy(c, dev::kCopyScatter, in, ist, out, ost, count * es, root, es);
+    case kGather: return launch_copy(c, dev::kCopyGather, in, ist, out, ost, count * es, root, es);
+    }
+    return fail(BINE_ERR_ARG, "unknown collective");
+}
+
+int plan_for_query(bine_comm_t c, int coll, long count, int root, std::shared_ptr<Schedule>* s) {
+    if (!c) return fail(BINE_ERR_ARG, "null communicator");
+    if (coll < 0 || coll >= kNumColls) return fail(BINE_ERR_ARG, "invalid collective");
+    if (count <= 0) return fail(BINE_ERR_ARG, "count must be positive");
+    return get_schedule(c, make_key(c, coll, count, root), s);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bine_last_error_string(void) { return g_err.c_str(); }
+
+int bine_comm_create(int nranks, int ndims, const int* dims, bine_comm_t* comm) {
+    if (!comm) return fail(BINE_ERR_ARG, "null output pointer");
+    *comm = nullptr;
+    if (nranks < 1 || nranks > (1 << 20)) return fail(BINE_ERR_ARG, "nranks must be in [1, 2^20]");
+    if (ndims < 0 || ndims > kMaxDims) return fail(BINE_ERR_ARG, "ndims must be in [0, 3] (lib/libbine.cc:131)");
+    long long prod = 1;
+    for (int i = 0; i < ndims; i++) {
+        if (!dims || dims[i] < 2) return fail(BINE_ERR_ARG, "every torus dimension must be at least 2");
+        prod *= dims[i];
+    }
+    if (ndims > 0 && prod != nranks) return fail(BINE_ERR_ARG, "dims do not multiply to nranks");
+    Torus t;
+    int d1[1] = {nranks};
+    t.init(ndims > 0 ? ndims : 1, ndims > 0 ? dims : d1);
+    if (t.num_steps > kMaxSteps) return fail(BINE_ERR_ARG, "too many steps for the distance tables");
+    bine_comm_t c = new bine_comm_s();
+    c->P = nranks;
+    c->planner.reset(new Planner(nranks, ndims, dims));
+    for (int i = 0; i < kNumColls; i++) c->cfg[i] = kDefaults[i];
+    *comm = c;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_destroy(bine_comm_t comm) {
+    if (!comm) return BINE_SUCCESS;
+    if (comm->device >= 0) cudaStreamSynchronize(comm->stream);
+    delete comm;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_stream(bine_comm_t comm, void* stream) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    comm->stream = (cudaStream_t)stream;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_layout(bine_comm_t comm, size_t send_stride, size_t recv_stride) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    comm->send_stride = send_stride;
+    comm->recv_stride = recv_stride;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_ports(bine_comm_t comm, int ports) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (ports < 1 || ports > kMaxPorts) return fail(BINE_ERR_ARG, "ports must be in [1, 6] (lib/libbine.cc:98)");
+    comm->ports = ports;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int family, int distance) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if ((int)coll < 0 || (int)coll >= kNumColls) return fail(BINE_ERR_ARG, "invalid collective");
+    if (family != BINE_FAMILY_BINE && family != BINE_FAMILY_RECDOUB) return fail(BINE_ERR_ARG, "invalid family");
+    if (distance != BINE_DISTANCE_DEFAULT && distance != kIncreasing && distance != kDecreasing)
+        return fail(BINE_ERR_ARG, "invalid distance");
+    static const int valid[kNumColls][4] = {{kArL, kArB, kArBCont, kArBCoalesce},
+                                             {kRsContPermute, -1, -1, -1},
+                                             {kAgContPermute, kAgContSend, kAgBlocks, -1},
+                                             {kBcTree, kBcScatterAllgather, -1, -1},
+                                             {kRdTree, kRdRedscatGather, -1, -1},
+                                             {kA2aLog, -1, -1, -1},
+                                             {kScTree, -1, -1, -1},
+                                             {kGaTree, -1, -1, -1}};
+    bool ok = false;
+    for (int v : valid[coll]) ok |= v == variant;
+    if (!ok) return fail(BINE_ERR_ARG, "invalid variant for this collective");
+    CollCfg cf;
+    cf.variant = variant;
+    cf.family = family;
+    cf.distance = distance == BINE_DISTANCE_DEFAULT ? kDefaults[coll].distance : distance;
+    // Scatter-allgather bcast runs with INCREASING distance (lib/libbine.cc:1267).
+    if (coll == BINE_COLL_BCAST && variant == kBcScatterAllgather && distance == BINE_DISTANCE_DEFAULT)
+        cf.distance = kIncreasing;
+    comm->cfg[coll] = cf;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_engine(bine_comm_t comm, int engine) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (engine != BINE_ENGINE_FUSED && engine != BINE_ENGINE_STEPS) return fail(BINE_ERR_ARG, "invalid engine");
+    comm->engine = engine;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_float_order(bine_comm_t comm, int order) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (order != BINE_ORDER_REFERENCE && order != BINE_ORDER_FAST) return fail(BINE_ERR_ARG, "invalid order");
+    comm->order = order;
+    return BINE_SUCCESS;
+}
+
+int bine_allreduce(const void* sendbuf, void* recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
+                   bine_comm_t comm) {
+    if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
+    return run_collective(comm, kAllreduce, sendbuf, recvbuf, count, datatype, 0);
+}
+
+int bine_reduce_scatter(const void* sendbuf, void* recvbuf, const int* recvcounts, bine_datatype_t datatype,
+                        bine_op_t op, bine_comm_t comm) {
+    if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
+    if (!comm || !recvcounts) return fail(BINE_ERR_ARG, "null argument");
+    for (int i = 1; i < comm->P; i++)
+        if (recvcounts[i] != recvcounts[0])
+            return fail(BINE_ERR_UNSUPPORTED, "recvcounts must be equal (reduce_scatter_block semantics, lib/libbine.cc:1065)");
+    return run_collective(comm, kReduceScatter, sendbuf, recvbuf, recvcounts[0], datatype, 0);
+}
+
+int bine_allgather(const void* sendbuf, int sendcount, bine_datatype_t sendtype, void* recvbuf, int recvcount,
+                   bine_datatype_t recvtype, bine_comm_t comm) {
+    if (sendcount != recvcount || sendtype != recvtype)
+        return fail(BINE_ERR_UNSUPPORTED, "sendcount/type must equal recvcount/type (lib/libbine.cc:1170-1171)");
+    return run_collective(comm, kAllgather, sendbuf, recvbuf, sendcount, sendtype, 0);
+}
+
+int bine_bcast(void* buffer, int count, bine_datatype_t datatype, int root, bine_comm_t comm) {
+    return run_collective(comm, kBcast, nullptr, buffer, count, datatype, root);
+}
+
+int bine_alltoall(const void* sendbuf, int sendcount, bine_datatype_t sendtype, void* recvbuf, int recvcount,
+                  bine_datatype_t recvtype, bine_comm_t comm) {
+    if (sendcount != recvcount || sendtype != recvtype)
+        return fail(BINE_ERR_UNSUPPORTED, "sendcount/type must equal recvcount/type");
+    return run_collective(comm, kAlltoall, sendbuf, recvbuf, sendcount, sendtype, 0);
+}
+
+int bine_scatter(const void* sendbuf, int sendcount, bine_datatype_t sendtype, void* recvbuf, int recvcount,
+                 bine_datatype_t recvtype, int root, bine_comm_t comm) {
+    if (sendcount != recvcount || sendtype != recvtype)
+        return fail(BINE_ERR_UNSUPPORTED, "sendcount/type must equal recvcount/type (lib/libbine_coll_scatter.cc:197-198)");
+    return run_collective(comm, kScatter, sendbuf, recvbuf, recvcount, recvtype, root);
+}
+
+int bine_gather(const void* sendbuf, int sendcount, bine_datatype_t sendtype, void* recvbuf, int recvcount,
+                bine_datatype_t recvtype, int root, bine_comm_t comm) {
+    if (sendcount != recvcount || sendtype != recvtype)
+        return fail(BINE_ERR_UNSUPPORTED, "sendcount/type must equal recvcount/type (lib/libbine_coll_gather.cc:210)");
+    return run_collective(comm, kGather, sendbuf, recvbuf, sendcount, sendtype, root);
+}
+
+int bine_reduce(const void* sendbuf, void* recvbuf, int count, bine_datatype_t datatype, bine_op_t op, int root,
+                bine_comm_t comm) {
+    if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
+    return run_collective(comm, kReduce, sendbuf, recvbuf, count, datatype, root);
+}
+
+int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (timeout_ms == 0) return fail(BINE_ERR_ARG, "timeout must be positive");
+    comm->step_timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
+    return BINE_SUCCESS;
+}
+
+int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    comm->barrier_extra = extra;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_synchronize(bine_comm_t comm) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (comm->device < 0) return BINE_SUCCESS;
+    CUDA_TRY(cudaStreamSynchronize(comm->stream));
+    int st = 0;
+    CUDA_TRY(cudaMemcpy(&st, comm->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != dev::kStepOk) {
+        CUDA_TRY(cudaMemset(comm->status, 0, sizeof(int)));
+        return fail(BINE_ERR_TIMEOUT, "a grid barrier of the step engine timed out");
+    }
+    return BINE_SUCCESS;
+}
+
+int bine_plan_stats(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t out[5]) {
+    std::shared_ptr<Schedule> s;
+    int rc = plan_for_query(comm, coll, count, root, &s);
+    if (rc) return rc;
+    int64_t moves = 0, traffic = 0;
+    for (const auto& l : s->levels)
+        for (const Move& m : l) {
+            moves++;
+            traffic += m.n * (m.add ? 3 : 2);
+        }
+    out[0] = (int64_t)s->levels.size();
+    out[1] = moves;
+    out[2] = (int64_t)s->messages.size();
+    out[3] = s->tmp_elems;
+    out[4] = traffic;
+    return BINE_SUCCESS;
+}
+
+int bine_plan_moves(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t* moves, int64_t* sizes,
+                    size_t cap, size_t* n_moves) {
+    std::shared_ptr<Schedule> s;
+    int rc = plan_for_query(comm, coll, count, root, &s);
+    if (rc) return rc;
+    size_t i = 0;
+    for (size_t l = 0; l < s->levels.size(); l++)
+        for (const Move& m : s->levels[l]) {
+            if (i < cap && moves && sizes) {
+                int64_t* o = moves + 10 * i;
+                o[0] = (int64_t)l;
+                o[1] = m.dst.rank, o[2] = m.dst.buf, o[3] = m.dst.off;
+                o[4] = m.a.rank, o[5] = m.a.buf, o[6] = m.a.off;
+                o[7] = m.b.rank, o[8] = m.b.buf, o[9] = m.b.off;
+                sizes[i] = m.n * 2 + m.add;
+            }
+            i++;
+        }
+    if (n_moves) *n_moves = i;
+    return BINE_SUCCESS;
+}
+
+int bine_plan_messages(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t* msgs, size_t cap,
+                       size_t* n_msgs) {
+    std::shared_ptr<Schedule> s;
+    int rc = plan_for_query(comm, coll, count, root, &s);
+    if (rc) return rc;
+    for (size_t i = 0; i < s->messages.size() && i < cap && msgs; i++) {
+        const Message& m = s->messages[i];
+        msgs[4 * i] = m.level;
+        msgs[4 * i + 1] = m.src;
+        msgs[4 * i + 2] = m.dst;
+        msgs[4 * i + 3] = m.elems;
+    }
+    if (n_msgs) *n_msgs = s->messages.size();
+    return BINE_SUCCESS;
+}
+
+int bine_plan_trees(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t* prog, size_t prog_cap,
+                    size_t* n_prog, int64_t* segs, size_t seg_cap, size_t* n_segs) {
+    std::shared_ptr<Schedule> s;
+    int rc = plan_for_query(comm, coll, count, root, &s);
+    if (rc) return rc;
+    TreePlan tp;
+    std::string err;
+    if (!comm->planner->trees(make_key(comm, coll, count, root), *s, &tp, &err)) return fail(BINE_ERR_INTERNAL, err);
+    for (size_t i = 0; i < tp.prog.size() && i < prog_cap && prog; i++) {
+        prog[3 * i] = tp.prog[i].rank;
+        prog[3 * i + 1] = tp.prog[i].adds;
+        prog[3 * i + 2] = tp.prog[i].shift;
+    }
+    for (size_t i = 0; i < tp.segs.size() && i < seg_cap && segs; i++) {
+        const OutSegment& g = tp.segs[i];
+        int64_t* o = segs + 6 * i;
+        o[0] = g.off, o[1] = g.n, o[2] = g.rank, o[3] = g.prog_begin, o[4] = g.prog_len, o[5] = g.depth;
+    }
+    if (n_prog) *n_prog = tp.prog.size();
+    if (n_segs) *n_segs = tp.segs.size();
+    return BINE_SUCCESS;
+}
+
+int bine_link_bytes_host(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                         uint64_t* link_bytes, size_t cap) {
+    std::shared_ptr<Schedule> s;
+    int rc = plan_for_query(comm, coll, count, root, &s);
+    if (rc) return rc;
+    const int es = dtype_size(datatype);
+    if (es < 0) return fail(BINE_ERR_ARG, "invalid datatype");
+    std::vector<uint64_t> lb;
+    std::string err;
+    if (!bine::link_bytes(comm->planner->torus(), s->messages, es, &lb, &err)) return fail(BINE_ERR_INTERNAL, err);
+    if (cap < lb.size()) return fail(BINE_ERR_ARG, "link_bytes array too small");
+    std::copy(lb.begin(), lb.end(), link_bytes);
+    return BINE_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,478 @@
+// Device kernels of the Bine engine (sm_100a).
+//
+// All collectives here move or add whole rows of P virtual ranks that live
+// in one HBM: the work is streaming integer/float traffic, bound by HBM
+// bandwidth, so the kernels are built around 16-byte vector loads and
+// stores, enough independent loads in flight per thread to cover DRAM
+// latency (8 ranks per batch), streaming cache hints, and grids sized to the
+// 148 SMs.  Nothing here is a dense contraction, so there are no tensor-core
+// paths.
+//
+//   k_sum_*      fused reductions (allreduce, reduce_scatter, reduce): each
+//                column of the P inputs is read once and the result written
+//                once per destination; integer sums wrap exactly, the FAST
+//                float order accumulates in FP64.
+//   k_tree_*     fused reductions in the reference's exact float order: each
+//                output segment carries the postfix program of its addition
+//                tree (produced by the host planner), evaluated per column
+//                with an in-register top of stack.
+//   k_copy_*     allgather, bcast, alltoall, scatter and gather as one pass of
+//                16-byte copies (one load, one or P stores).
+//   k_steps      the reference's schedule executed level by level in one
+//                cooperative launch, with a bounded grid-wide barrier between
+//                levels that reports a timeout instead of hanging.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bine {
+namespace dev {
+
+constexpr int kThreads = 256;
+constexpr int kMaxTreeDepth = 24;
+
+// ---------------------------------------------------------------- memory
+__device__ __forceinline__ uint4 ld_stream(const void* p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+// L2-coherent load (bypasses L1): rows written by other blocks earlier in
+// the same launch must not be served from a stale L1 line.
+__device__ __forceinline__ uint4 ld_plain(const void* p) {
+    uint4 v;
+    asm volatile("ld.global.cg.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p)
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_stream(void* p, uint4 v) {
+    asm volatile("st.global.cs.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+                 : "memory");
+}
+
+// ----------------------------------------------------------- lane algebra
+// Accumulators: wrapping integers of the element type, FP64 for the FAST
+// float order, the element type itself for the exact float order.
+template <typename T>
+struct AccOf {
+    using type = T;
+};
+template <>
+struct AccOf<float> {
+    using type = double;
+};
+
+template <typename T>
+__device__ __forceinline__ T add_exact(T a, T b) {
+    return (T)(a + b);
+}
+template <>
+__device__ __forceinline__ float add_exact<float>(float a, float b) {
+    return __fadd_rn(a, b);
+}
+template <>
+__device__ __forceinline__ double add_exact<double>(double a, double b) {
+    return __dadd_rn(a, b);
+}
+
+template <typename T, typename A>
+struct Lanes {
+    static constexpr int N = 16 / sizeof(T);
+    A v[N];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < N; i++) v[i] = (A)0;
+    }
+    __device__ __forceinline__ void add(uint4 raw) {
+        const T* t = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+        for (int i = 0; i < N; i++) v[i] = add_exact<A>(v[i], (A)t[i]);
+    }
+    __device__ __forceinline__ uint4 pack() const {
+        uint4 raw;
+        T* t = reinterpret_cast<T*>(&raw);
+#pragma unroll
+        for (int i = 0; i < N; i++) t[i] = (T)v[i];
+        return raw;
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ uint4 vadd(uint4 a, uint4 b) {
+    uint4 r;
+    const T* x = reinterpret_cast<const T*>(&a);
+    const T* y = reinterpret_cast<const T*>(&b);
+    T* z = reinterpret_cast<T*>(&r);
+#pragma unroll
+    for (int i = 0; i < (int)(16 / sizeof(T)); i++) z[i] = add_exact<T>(x[i], y[i]);
+    return r;
+}
+
+// ------------------------------------------------------- fused reductions
+enum SumMode { kSumAllreduce = 0, kSumReduceScatter = 1, kSumReduce = 2 };
+
+// Column sums over 16-byte vector columns.  `ncol` vector columns per input
+// row; reduce_scatter: `blk` vector columns per destination rank.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads) k_sum_vec(const char* __restrict__ in, long long in_stride,
+                                                      char* __restrict__ out, long long out_stride, int P,
+                                                      long long ncol, long long blk, int root) {
+    using A = typename AccOf<T>::type;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += step) {
+        Lanes<T, A> acc;
+        acc.zero();
+        const char* p = in + col * 16;
+        int r = 0;
+        for (; r + 8 <= P; r += 8) {
+            uint4 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = ld_stream(p + (long long)(r + u) * in_stride);
+#pragma unroll
+            for (int u = 0; u < 8; u++) acc.add(v[u]);
+        }
+        for (; r < P; r++) acc.add(ld_stream(p + (long long)r * in_stride));
+        const uint4 res = acc.pack();
+        if (MODE == kSumAllreduce) {
+            char* q = out + col * 16;
+            for (int d = 0; d < P; d++) st_stream(q + (long long)d * out_stride, res);
+        } else if (MODE == kSumReduceScatter) {
+            long long owner = col / blk;
+            st_stream(out + owner * out_stride + (col - owner * blk) * 16, res);
+        } else {
+            st_stream(out + (long long)root * out_stride + col * 16, res);
+        }
+    }
+}
+
+// Element-wise fallback for unaligned layouts and tails: elements
+// [e0, e0 + n) of every row.  reduce_scatter: `blk` elements per rank.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads) k_sum_scalar(const char* __restrict__ in, long long in_stride,
+                                                         char* __restrict__ out, long long out_stride, int P,
+                                                         long long e0, long long n, long long blk, int root) {
+    using A = typename AccOf<T>::type;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
+        const long long e = e0 + i;
+        A acc = (A)0;
+        for (int r = 0; r < P; r++) acc = add_exact<A>(acc, (A) * (const T*)(in + (long long)r * in_stride + e * sizeof(T)));
+        const T res = (T)acc;
+        if (MODE == kSumAllreduce) {
+            for (int d = 0; d < P; d++) *(T*)(out + (long long)d * out_stride + e * sizeof(T)) = res;
+        } else if (MODE == kSumReduceScatter) {
+            long long owner = e / blk;
+            *(T*)(out + owner * out_stride + (e - owner * blk) * sizeof(T)) = res;
+        } else {
+            *(T*)(out + (long long)root * out_stride + e * sizeof(T)) = res;
+        }
+    }
+}
+
+// ------------------------------------------- fused reductions, exact order
+struct TreeEntry {  // one postfix entry: push input (rank, out + shift), then `adds` additions
+    int32_t rank;
+    int32_t adds;
+    int64_t shift;
+};
+struct TreeSeg {  // output elements [off, off + n) of `rank` (-1: all ranks)
+    int64_t off, n;
+    int32_t rank, prog_begin, prog_len, depth;
+};
+struct TreeTile {  // `n` elements starting `start` elements into segment `seg`
+    int32_t seg, pad;
+    int64_t start, n;
+};
+
+// Vector form: every shift and offset is a multiple of 16 bytes.  One tile
+// per block; each thread owns one 16-byte column of the tile.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ in, long long in_stride,
+                                                       char* __restrict__ out, long long out_stride, int P,
+                                                       const TreeSeg* __restrict__ segs,
+                                                       const TreeEntry* __restrict__ prog,
+                                                       const TreeTile* __restrict__ tiles, int ntiles) {
+    extern __shared__ TreeEntry sprog[];
+    constexpr int L = 16 / sizeof(T);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const TreeTile tile = tiles[t];
+        const TreeSeg sg = segs[tile.seg];
+        __syncthreads();
+        for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
+        __syncthreads();
+        const long long col = (long long)threadIdx.x * L;
+        if (col >= tile.n) continue;
+        const long long e = sg.off + tile.start + col;  // output element
+        uint4 stk[kMaxTreeDepth];
+        uint4 top = make_uint4(0, 0, 0, 0);
+        int sp = 0;
+        const int len = sg.prog_len;
+        // Loads run 8 entries ahead of the additions.
+        uint4 ring[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (u < len) {
+                const TreeEntry q = sprog[u];
+                ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+            }
+        for (int k0 = 0; k0 < len; k0 += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int k = k0 + u;
+                if (k < len) {
+                    const uint4 v = ring[u];
+                    if (k + 8 < len) {
+                        const TreeEntry q = sprog[k + 8];
+                        ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                    }
+                    if (k > 0) stk[sp++] = top;
+                    top = v;
+                    for (int a = sprog[k].adds; a > 0; a--) top = vadd<T>(stk[--sp], top);
+                }
+            }
+        }
+        if (sg.rank < 0) {
+            for (int d = 0; d < P; d++) st_stream(out + (long long)d * out_stride + e * (long long)sizeof(T), top);
+        } else {
+            st_stream(out + (long long)sg.rank * out_stride + e * (long long)sizeof(T), top);
+        }
+    }
+}
+
+// Element form for layouts that are not 16-byte aligned.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_tree_scalar(const char* __restrict__ in, long long in_stride,
+                                                          char* __restrict__ out, long long out_stride, int P,
+                                                          const TreeSeg* __restrict__ segs,
+                                                          const TreeEntry* __restrict__ prog,
+                                                          const TreeTile* __restrict__ tiles, int ntiles) {
+    extern __shared__ TreeEntry sprog[];
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const TreeTile tile = tiles[t];
+        const TreeSeg sg = segs[tile.seg];
+        __syncthreads();
+        for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
+        __syncthreads();
+        for (long long col = threadIdx.x; col < tile.n; col += blockDim.x) {
+            const long long e = sg.off + tile.start + col;
+            T stk[kMaxTreeDepth];
+            T top = (T)0;
+            int sp = 0;
+            for (int k = 0; k < sg.prog_len; k++) {
+                const TreeEntry q = sprog[k];
+                const T v = *(const T*)(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                if (k > 0) stk[sp++] = top;
+                top = v;
+                for (int a = q.adds; a > 0; a--) top = add_exact<T>(stk[--sp], top);
+            }
+            if (sg.rank < 0) {
+                for (int d = 0; d < P; d++) *(T*)(out + (long long)d * out_stride + e * (long long)sizeof(T)) = top;
+            } else {
+                *(T*)(out + (long long)sg.rank * out_stride + e * (long long)sizeof(T)) = top;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------- copies
+enum CopyMode { kCopyAllgather = 0, kCopyBcast = 1, kCopyAlltoall = 2, kCopyScatter = 3, kCopyGather = 4 };
+
+// A copy collective is a set of "pairs" (source row piece, destination row
+// pieces) of `unit` bytes each; unit = one rank's block.
+struct CopyArgs {
+    const char* in;
+    long long in_stride;
+    char* out;
+    long long out_stride;
+    int P;
+    int root;
+    long long unit;  // bytes per block
+};
+
+template <int MODE>
+__device__ __forceinline__ long long copy_pairs(const CopyArgs& a) {
+    if (MODE == kCopyAlltoall) return (long long)a.P * a.P;
+    if (MODE == kCopyBcast) return 1;
+    return a.P;
+}
+
+// Source of pair `i` and its destinations (first and count; bcast and
+// allgather broadcast one load to several rows).
+template <int MODE>
+__device__ __forceinline__ const char* copy_src(const CopyArgs& a, long long i) {
+    if (MODE == kCopyAllgather) return a.in + i * a.in_stride;
+    if (MODE == kCopyBcast) return a.in + (long long)a.root * a.in_stride;
+    if (MODE == kCopyAlltoall) {
+        long long src = i / a.P, dst = i % a.P;  // block dst of row src
+        return a.in + src * a.in_stride + dst * a.unit;
+    }
+    if (MODE == kCopyScatter) return a.in + (long long)a.root * a.in_stride + i * a.unit;
+    return a.in + i * a.in_stride;  // gather
+}
+template <int MODE>
+__device__ __forceinline__ int copy_ndst(const CopyArgs& a) {
+    if (MODE == kCopyAllgather) return a.P;
+    if (MODE == kCopyBcast) return a.P;
+    return 1;
+}
+template <int MODE>
+__device__ __forceinline__ char* copy_dst(const CopyArgs& a, long long i, int d) {
+    if (MODE == kCopyAllgather) return a.out + (long long)d * a.out_stride + i * a.unit;
+    if (MODE == kCopyBcast) return d == a.root ? nullptr : a.out + (long long)d * a.out_stride;
+    if (MODE == kCopyAlltoall) {
+        long long src = i / a.P, dst = i % a.P;
+        return a.out + dst * a.out_stride + src * a.unit;
+    }
+    if (MODE == kCopyScatter) return a.out + i * a.out_stride;
+    return a.out + (long long)a.root * a.out_stride + i * a.unit;  // gather
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) k_copy_vec(CopyArgs a) {
+    const long long nvec = a.unit / 16;
+    const long long total = copy_pairs<MODE>(a) * nvec;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += step) {
+        const long long i = w / nvec, j = w - (w / nvec) * nvec;
+        const uint4 v = ld_stream(copy_src<MODE>(a, i) + j * 16);
+        const int nd = copy_ndst<MODE>(a);
+        for (int d = 0; d < nd; d++) {
+            char* q = copy_dst<MODE>(a, i, d);
+            if (q) st_stream(q + j * 16, v);
+        }
+    }
+}
+
+template <int MODE, typename U>
+__global__ void __launch_bounds__(kThreads) k_copy_scalar(CopyArgs a) {
+    const long long nu = a.unit / (long long)sizeof(U);
+    const long long total = copy_pairs<MODE>(a) * nu;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += step) {
+        const long long i = w / nu, j = w - (w / nu) * nu;
+        const U v = *(const U*)(copy_src<MODE>(a, i) + j * sizeof(U));
+        const int nd = copy_ndst<MODE>(a);
+        for (int d = 0; d < nd; d++) {
+            char* q = copy_dst<MODE>(a, i, d);
+            if (q) *(U*)(q + j * sizeof(U)) = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------- step engine
+struct StepMove {
+    int64_t dst_off, a_off, b_off;  // elements
+    int32_t dst_rank, a_rank, b_rank;
+    uint8_t dst_buf, a_buf, b_buf, add;
+};
+struct StepChunk {  // elements [start, start + n) of move `move`
+    int32_t move, pad;
+    int64_t start, n;
+};
+struct StepBufs {
+    char* base[3];       // send, receive, workspace
+    long long stride[3];  // bytes between rank rows
+};
+
+enum StepStatus { kStepOk = 0, kStepTimeout = 1 };
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier for a cooperative launch.  bar[0] counts arrivals,
+// bar[1] is the generation; the last of `expected` arrivals (normally
+// gridDim.x) opens it.  The wait is bounded by `timeout_ns` of %globaltimer
+// and by an iteration cap; on expiry the block records kStepTimeout in
+// *status and returns false (the caller then exits, so the other blocks time
+// out too instead of waiting forever).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status, unsigned long long timeout_ns,
+                                             unsigned expected) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        __threadfence();
+        const unsigned gen = ld_acquire(&bar[1]);
+        const unsigned arrived = atomicAdd(&bar[0], 1u);
+        if (arrived == expected - 1) {
+            bar[0] = 0;
+            __threadfence();
+            st_release(&bar[1], gen + 1);
+        } else {
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned long long iters = 0;
+            while (ld_acquire(&bar[1]) == gen) {
+                if (++iters > (1ull << 40) || globaltimer_ns() - t0 > timeout_ns ||
+                    *(volatile int*)status != kStepOk) {
+                    atomicCAS(status, kStepOk, kStepTimeout);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <typename T>
+__device__ __forceinline__ void run_chunk(const StepBufs& B, const StepMove& m, const StepChunk& ch) {
+    constexpr long long es = sizeof(T);
+    char* d = B.base[m.dst_buf] + (long long)m.dst_rank * B.stride[m.dst_buf] + (m.dst_off + ch.start) * es;
+    const char* a = B.base[m.a_buf] + (long long)m.a_rank * B.stride[m.a_buf] + (m.a_off + ch.start) * es;
+    const char* b = B.base[m.b_buf] + (long long)m.b_rank * B.stride[m.b_buf] + (m.b_off + ch.start) * es;
+    const long long bytes = ch.n * es;
+    const bool vec = (((uintptr_t)d | (uintptr_t)a | (uintptr_t)(m.add ? b : a)) & 15) == 0 && (bytes & 15) == 0;
+    if (vec) {
+        const long long nv = bytes / 16;
+        for (long long i = threadIdx.x; i < nv; i += blockDim.x) {
+            // Plain (coherent) loads: earlier levels of this launch wrote
+            // these rows.
+            uint4 v = ld_plain(a + i * 16);
+            if (m.add) v = vadd<T>(v, ld_plain(b + i * 16));
+            *(uint4*)(d + i * 16) = v;
+        }
+    } else {
+        for (long long i = threadIdx.x; i < ch.n; i += blockDim.x) {
+            T v = ((volatile const T*)a)[i];
+            if (m.add) v = add_exact<T>(v, ((volatile const T*)b)[i]);
+            ((T*)d)[i] = v;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_steps(StepBufs B, const StepMove* __restrict__ moves,
+                                                    const StepChunk* __restrict__ chunks,
+                                                    const int* __restrict__ level_begin, int nlevels,
+                                                    unsigned* bar, int* status, unsigned long long timeout_ns,
+                                                    unsigned expected) {
+    for (int l = 0; l < nlevels; l++) {
+        for (int c = level_begin[l] + blockIdx.x; c < level_begin[l + 1]; c += gridDim.x) {
+            const StepChunk ch = chunks[c];
+            run_chunk<T>(B, moves[ch.move], ch);
+        }
+        if (l + 1 < nlevels && !grid_barrier(bar, status, timeout_ns, expected)) return;
+    }
+}
+
+}  // namespace dev
+}  // namespace bine

@@ -1,0 +1,149 @@
+// Host-side planner: turns one Bine collective (variant, P, torus, ports,
+// count) into a device-executable schedule.
+//
+// The schedule IR is a list of levels; each level is a set of moves that run
+// concurrently and read the state left by the previous level:
+//     dst = a           (copy)
+//     dst = a + b       (MPI_SUM; a and b may come from different ranks)
+// over regions (rank, buffer, element offset).  Buffers are the caller's
+// send and receive arrays and the communicator's workspace.  A message of the
+// reference (an MPI send matched with its receive) becomes one move reading
+// the sender's region directly, the way a kernel reads a peer's rows in HBM;
+// a receive followed by MPI_Reduce_local becomes one "dst = a + b" move.
+//
+// The IR feeds three consumers:
+//   * the persistent step kernel (bine_kernels.cu), level by level;
+//   * the symbolic executor below, which derives for every output element
+//     the exact addition tree the reference evaluates, so the fused kernels
+//     can reproduce float32 results bit for bit;
+//   * link-byte accounting on a torus (every message, routed minimally).
+#pragma once
+
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "bine_sched.h"
+
+namespace bine {
+
+enum BufId : uint8_t { kBufSend = 0, kBufRecv = 1, kBufTmp = 2, kNumBufs = 3 };
+
+enum Coll : int {
+    kAllreduce = 0,
+    kReduceScatter = 1,
+    kAllgather = 2,
+    kBcast = 3,
+    kReduce = 4,
+    kAlltoall = 5,
+    kScatter = 6,
+    kGather = 7,
+    kNumColls = 8
+};
+
+// Variant numbering follows the reference's per-collective algorithm enums
+// (lib/libbine_common.h:74-123).
+enum : int {
+    kArL = 0, kArB = 1, kArBCont = 3, kArBCoalesce = 4,
+    kAgContPermute = 0, kAgContSend = 1, kAgBlocks = 2,
+    kRsContPermute = 0, kRsBlocks = 2,
+    kBcTree = 0, kBcScatterAllgather = 2,
+    kRdTree = 0, kRdRedscatGather = 1,
+    kA2aLog = 0, kScTree = 0, kGaTree = 0
+};
+
+enum Distance : int { kIncreasing = 0, kDecreasing = 1 };
+
+struct Region {
+    int32_t rank;
+    uint8_t buf;
+    int64_t off;  // elements
+};
+
+struct Move {
+    Region dst, a, b;
+    int64_t n;    // elements
+    uint8_t add;  // 0: dst = a, 1: dst = a + b
+};
+
+struct Message {
+    int32_t level;
+    int32_t src, dst;
+    int64_t elems;
+};
+
+struct PlanKey {
+    int coll, variant, family, distance, ports, root;
+    int64_t count;
+    bool operator==(const PlanKey& o) const {
+        return coll == o.coll && variant == o.variant && family == o.family && distance == o.distance &&
+               ports == o.ports && root == o.root && count == o.count;
+    }
+};
+struct PlanKeyHash {
+    size_t operator()(const PlanKey& k) const {
+        size_t h = (size_t)k.count * 1000003u;
+        h ^= (size_t)k.coll * 31 + (size_t)k.variant * 131 + (size_t)k.family * 521 + (size_t)k.distance * 2053 +
+             (size_t)k.ports * 8191 + (size_t)(k.root + 7) * 131071;
+        return h;
+    }
+};
+
+struct Schedule {
+    std::vector<std::vector<Move>> levels;
+    std::vector<Message> messages;
+    int64_t send_elems = 0, recv_elems = 0;  // per rank
+    int64_t tmp_elems = 0;                   // workspace elements per rank
+};
+
+// One reduction tree in postfix form: leaves are (rank, input shift), each
+// followed by `adds` additions of the two top stack entries.
+struct ProgEntry {
+    int32_t rank;
+    int32_t adds;
+    int64_t shift;  // input element = output element + shift
+};
+
+// A run of output elements [off, off + n) on rank `rank` (-1: every rank)
+// whose value is the program prog[begin, begin + len).
+struct OutSegment {
+    int64_t off, n;
+    int32_t rank;
+    int32_t prog_begin, prog_len;
+    int32_t depth;  // evaluation stack depth of the program
+};
+
+struct TreePlan {
+    std::vector<ProgEntry> prog;
+    std::vector<OutSegment> segs;
+    int max_depth = 0;
+};
+
+class Planner {
+  public:
+    Planner(int nranks, int ndims, const int* dims);
+    const Torus& torus() const { return t_; }
+
+    // Builds the schedule of one call.  Returns false with `err` set when the
+    // reference cannot run this case (it asserts, exits, deadlocks, corrupts
+    // memory or returns wrong data); `err` names the reference line.
+    bool build(const PlanKey& k, Schedule* out, std::string* err) const;
+
+    // Exact reduction trees of every output element (float reference order).
+    bool trees(const PlanKey& k, const Schedule& s, TreePlan* out, std::string* err) const;
+
+  private:
+    Torus t_;
+};
+
+// Per-link byte counts of a message list on the torus: 2 * ndims directed
+// links per node, index (node * ndims + d) * 2 + (dir > 0 ? 0 : 1).
+// Returns false if some message moves along more than one dimension.
+bool link_bytes(const Torus& t, const std::vector<Message>& msgs, int elem_size, std::vector<uint64_t>* out,
+                std::string* err);
+
+}  // namespace bine

@@ -1,0 +1,211 @@
+/*
+ * bine_b200.h -- C ABI of the B200 engine for the Bine-tree collectives.
+ *
+ * A communicator holds P "virtual ranks" whose buffers all live in the HBM of
+ * one GPU.  Every buffer argument is a DEVICE pointer to a rank-major array:
+ * rank r's row starts at  base + r * stride  bytes.  By default the stride is
+ * the row size (rows packed back to back); bine_comm_set_layout() sets a
+ * larger one.  Calls are asynchronous and ordered on the communicator's CUDA
+ * stream.  Functions return BINE_SUCCESS or an error code and never abort;
+ * bine_last_error_string() describes the last error of the calling thread.
+ *
+ * The eight collectives keep the argument lists of the reference library's
+ * MPI entry points (HLC-Lab/bine_trees_fugaku, lib/libbine.cc): one call here
+ * performs the collective for all P ranks at once.  Algorithm selection
+ * mirrors the reference's LIBBINE_* environment variables
+ * (lib/libbine.cc:75-575) as explicit per-communicator settings.
+ */
+#ifndef BINE_B200_H
+#define BINE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bine_comm_s *bine_comm_t;
+
+/* Element types (MPI_INT32_T, MPI_INT64_T, MPI_FLOAT, MPI_DOUBLE, MPI_CHAR). */
+typedef enum {
+    BINE_INT32 = 0,
+    BINE_INT64 = 1,
+    BINE_FLOAT = 2,
+    BINE_DOUBLE = 3,
+    BINE_CHAR = 4
+} bine_datatype_t;
+
+/* Reduction operators (MPI_SUM). */
+typedef enum { BINE_SUM = 0 } bine_op_t;
+
+/* Return codes. */
+enum {
+    BINE_SUCCESS = 0,
+    BINE_ERR_ARG = 1,         /* invalid argument */
+    BINE_ERR_UNSUPPORTED = 2, /* the selected reference algorithm cannot run this case */
+    BINE_ERR_CUDA = 3,        /* a CUDA call failed */
+    BINE_ERR_TIMEOUT = 4,     /* a bounded device-side wait expired */
+    BINE_ERR_NOMEM = 5,       /* device memory exhausted */
+    BINE_ERR_INTERNAL = 6
+};
+
+/* Collectives, for bine_comm_set_algo() and the planning queries. */
+typedef enum {
+    BINE_COLL_ALLREDUCE = 0,
+    BINE_COLL_REDUCE_SCATTER = 1,
+    BINE_COLL_ALLGATHER = 2,
+    BINE_COLL_BCAST = 3,
+    BINE_COLL_REDUCE = 4,
+    BINE_COLL_ALLTOALL = 5,
+    BINE_COLL_SCATTER = 6,
+    BINE_COLL_GATHER = 7
+} bine_coll_t;
+
+/* Algorithm variants: the values of the reference's LIBBINE_<COLL>_ALGO
+ * (enums at lib/libbine_common.h:74-123). */
+enum {
+    BINE_ALLREDUCE_L = 0, BINE_ALLREDUCE_B = 1, BINE_ALLREDUCE_B_CONT = 3, BINE_ALLREDUCE_B_COALESCE = 4,
+    BINE_ALLGATHER_CONT_PERMUTE = 0, BINE_ALLGATHER_CONT_SEND = 1, BINE_ALLGATHER_BLOCKS = 2,
+    BINE_REDUCE_SCATTER_CONT_PERMUTE = 0,
+    BINE_BCAST_BINOMIAL_TREE = 0, BINE_BCAST_SCATTER_ALLGATHER = 2,
+    BINE_REDUCE_BINOMIAL_TREE = 0, BINE_REDUCE_SCATTER_GATHER = 1,
+    BINE_ALLTOALL_LOG = 0, BINE_SCATTER_BINOMIAL_TREE = 0, BINE_GATHER_BINOMIAL_TREE = 0
+};
+
+/* LIBBINE_<COLL>_ALGO_FAMILY and LIBBINE_<COLL>_DISTANCE. */
+enum { BINE_FAMILY_BINE = 1, BINE_FAMILY_RECDOUB = 2 };
+enum { BINE_DISTANCE_INCREASING = 0, BINE_DISTANCE_DECREASING = 1, BINE_DISTANCE_DEFAULT = -1 };
+
+/* Execution engines.
+ *   FUSED (default): one kernel per call that reads every input element
+ *     once and writes every output element once, evaluating the reference's
+ *     exact addition tree per element in registers;
+ *   STEPS: one persistent kernel that executes the reference's schedule step
+ *     by step (the message pattern of the MPI layer, as device loads and
+ *     stores), with a bounded grid-wide barrier between steps. */
+enum { BINE_ENGINE_FUSED = 0, BINE_ENGINE_STEPS = 1 };
+
+/* Floating-point summation order for the FUSED engine.
+ *   REFERENCE (default): bit-identical to the reference's per-step order;
+ *   FAST: straight column sums accumulated in FP64 and rounded once. */
+enum { BINE_ORDER_REFERENCE = 0, BINE_ORDER_FAST = 1 };
+
+/* ---------------------------------------------------------- communicator */
+
+/* Creates a communicator of `nranks` virtual ranks on the current device,
+ * arranged as a torus of `ndims` (0..3) dimensions `dims` (ndims = 0: one
+ * ring of nranks).  Replaces MPI_COMM_WORLD plus LIBBINE_DIMENSIONS
+ * (lib/libbine.cc:114-130).  No device memory is touched until the first
+ * collective. */
+int bine_comm_create(int nranks, int ndims, const int *dims, bine_comm_t *comm);
+int bine_comm_destroy(bine_comm_t comm);
+
+/* CUDA stream (a cudaStream_t) the calls are ordered on; NULL = default. */
+int bine_comm_set_stream(bine_comm_t comm, void *stream);
+
+/* Bytes between consecutive rank rows of the send and receive arrays; 0
+ * keeps rows packed.  Strides must cover the row sizes of each call. */
+int bine_comm_set_layout(bine_comm_t comm, size_t send_stride, size_t recv_stride);
+
+/* LIBBINE_NUM_PORTS (1..6). */
+int bine_comm_set_ports(bine_comm_t comm, int ports);
+
+/* LIBBINE_<COLL>_ALGO, _ALGO_FAMILY and _DISTANCE for one collective. */
+int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int family, int distance);
+
+int bine_comm_set_engine(bine_comm_t comm, int engine);
+int bine_comm_set_float_order(bine_comm_t comm, int order);
+
+/* ----------------------------------------------------------- collectives */
+
+/* MPI_Allreduce, lib/libbine.cc:1012. */
+int bine_allreduce(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
+                   bine_comm_t comm);
+
+/* MPI_Reduce_scatter, lib/libbine.cc:1064 (recvcounts must all be equal, as
+ * the reference's block implementation assumes, lib/libbine.cc:1065). */
+int bine_reduce_scatter(const void *sendbuf, void *recvbuf, const int *recvcounts, bine_datatype_t datatype,
+                        bine_op_t op, bine_comm_t comm);
+
+/* MPI_Allgather, lib/libbine.cc:1168 (sendcount == recvcount and
+ * sendtype == recvtype, lib/libbine.cc:1170-1171). */
+int bine_allgather(const void *sendbuf, int sendcount, bine_datatype_t sendtype, void *recvbuf, int recvcount,
+                   bine_datatype_t recvtype, bine_comm_t comm);
+
+/* MPI_Bcast_f, lib/libbine.cc:1252: in place on `buffer`; the root's row
+ * holds the data. */
+int bine_bcast(void *buffer, int count, bine_datatype_t datatype, int root, bine_comm_t comm);
+
+/* MPI_Alltoall, lib/libbine.cc:1291. */
+int bine_alltoall(const void *sendbuf, int sendcount, bine_datatype_t sendtype, void *recvbuf, int recvcount,
+                  bine_datatype_t recvtype, bine_comm_t comm);
+
+/* MPI_Scatter, lib/libbine.cc:1312 (only the root's send row is read). */
+int bine_scatter(const void *sendbuf, int sendcount, bine_datatype_t sendtype, void *recvbuf, int recvcount,
+                 bine_datatype_t recvtype, int root, bine_comm_t comm);
+
+/* MPI_Gather, lib/libbine.cc:1376 (only the root's receive row is written). */
+int bine_gather(const void *sendbuf, int sendcount, bine_datatype_t sendtype, void *recvbuf, int recvcount,
+                bine_datatype_t recvtype, int root, bine_comm_t comm);
+
+/* MPI_Reduce, lib/libbine.cc:1440 (only the root's receive row is written). */
+int bine_reduce(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op, int root,
+                bine_comm_t comm);
+
+/* Waits for the communicator's stream and reports device-side errors
+ * (BINE_ERR_TIMEOUT when a bounded barrier of the STEPS engine expired). */
+int bine_comm_synchronize(bine_comm_t comm);
+
+const char *bine_last_error_string(void);
+
+/* Bound of every device-side wait of the STEPS engine (grid barriers between
+ * steps), in milliseconds; default 5000.  A wait that expires makes the
+ * kernel record the timeout and return; bine_comm_synchronize() then
+ * reports BINE_ERR_TIMEOUT and the context stays usable. */
+int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms);
+
+/* Fault injection for tests of the timeout path: makes every grid barrier of
+ * the STEPS engine wait for `extra` arrivals that never come, so the bounded
+ * wait expires (0 restores normal operation).  Nothing faults or hangs. */
+int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
+
+/* ------------------------------------------------------ schedule queries
+ * Host-only: these plan the call with the communicator's current settings
+ * and need no GPU.  `count` and `root` have the meaning of the collective's
+ * own arguments (for reduce_scatter, the per-rank receive count). */
+
+/* Sizes of the schedule: out[0] = steps (levels), out[1] = moves,
+ * out[2] = messages, out[3] = workspace elements per rank,
+ * out[4] = bytes read + written by the STEPS engine per element size. */
+int bine_plan_stats(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t out[5]);
+
+/* The schedule's moves, level by level.  Each move is 10 int64 values:
+ * level, dst_rank, dst_buf, dst_off, a_rank, a_buf, a_off, b_rank, b_buf,
+ * b_off (buffers: 0 send, 1 receive, 2 workspace; offsets in elements), and
+ * a parallel array gives n and whether it adds (n * 2 + add). */
+int bine_plan_moves(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t *moves, int64_t *sizes,
+                    size_t cap, size_t *n_moves);
+
+/* The reference's messages of the call: (level, src, dst, elements). */
+int bine_plan_messages(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t *msgs, size_t cap,
+                       size_t *n_msgs);
+
+/* Exact reduction trees (allreduce, reduce_scatter, reduce): postfix
+ * programs of (rank, adds, shift) entries and output segments of
+ * (offset, n, rank (-1: all), program begin, program length, depth). */
+int bine_plan_trees(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t *prog, size_t prog_cap,
+                    size_t *n_prog, int64_t *segs, size_t seg_cap, size_t *n_segs);
+
+/* Per-link byte counts of the call's messages on the communicator's torus
+ * (minimal ring routes; 2*ndims directed links per rank, index
+ * (rank*ndims + d)*2 + (0: + direction, 1: - direction)).  Computed on the
+ * host from the planned schedule. */
+int bine_link_bytes_host(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                         uint64_t *link_bytes, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BINE_B200_H */
