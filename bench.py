@@ -1,0 +1,347 @@
+#!/usr/bin/env python3
+"""Benchmark of the Bine engine on B200: virtual-rank Bine allreduce GB/s.
+
+Workload (one "step"): Bine allreduce (variant B, one port, 1-D ring) over
+P = 256 virtual ranks, 1,048,576 int32 per rank (4 MiB), values uniform in
+[-1000, 1000] from a seed, MPI_SUM -- every rank ends with the full sum.
+The inputs (1 GiB) and results (1 GiB) are larger than the 126 MB L2, so no
+L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Engine arm (default): K steps of bine_allreduce with the buffers resident in
+HBM, bracketed by a barrier and torch.cuda.synchronize(), timed with CUDA
+events on the engine's stream; max over ranks when launched with torchrun
+(N independent replicas: a collective over virtual ranks does not shard
+across GPUs).  The JSON line also carries the HBM roofline of the fused
+kernel, the end-to-end figure through the C ABI with host buffers, the
+reference's CPU time on this host (cpu_baseline), and the SM clocks sampled
+during the timed region.
+
+Reference arm (--impl reference): the reference library itself, built from
+its sources against the project's MPI shim (oracle/_ref), one forked process
+per virtual rank on this host's cores, timed as bench/bench.cc does.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P_RANKS = 256
+COUNT = 1 << 20  # int32 per rank: 4 MiB
+ES = 4
+ALGO_BYTES = 2 * P_RANKS * COUNT * ES  # every input read once, every output written once
+
+
+def configure(args):
+    """Applies the profiling overrides (--P/--count/--dtype/--engine/--order);
+    the defaults are the benchmark workload."""
+    global P_RANKS, COUNT, ES, ALGO_BYTES, WORKLOAD
+    P_RANKS, COUNT = args.P, args.count
+    ES = 4
+    ALGO_BYTES = 2 * P_RANKS * COUNT * ES
+    if (args.P, args.count, args.dtype, args.engine) != (256, 1 << 20, "int32", "fused"):
+        WORKLOAD = (f"Bine allreduce (variant B, 1 port, 1-D ring), P={P_RANKS} virtual ranks, {COUNT} {args.dtype} "
+                    f"per rank, MPI_SUM, {args.engine} engine, {args.order} float order (profiling variant)")
+METRIC = "virtual-rank Bine allreduce GB/s"
+WORKLOAD = "Bine allreduce (variant B, 1 port, 1-D ring), P=256 virtual ranks, 1,048,576 int32 (4 MiB) per rank, MPI_SUM"
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "allreduce_fused_p256_4MiB_int32.txt")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    if not os.path.exists(PROFILE_SUMMARY):
+        return None
+    with open(PROFILE_SUMMARY) as f:
+        for line in f:
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(float(line.split(":", 1)[1]))
+    return None
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"],
+                                 parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_time(steps, warmup, budget_s=150.0):
+    """Times the reference library (oracle/_ref) on this host; returns a dict."""
+    from oracle import ref
+
+    if not ref.available():
+        return None
+    count = COUNT
+    # Calibrate one call at full size, then shrink the per-step sample only
+    # if K calls would not fit in the time budget.
+    probe = ref.time_collective("allreduce", "int32", count, P_RANKS, iters=1, warmup=0, timeout=600)
+    if not probe.get("ok"):
+        return {"error": "reference run failed", "detail": probe}
+    t_call = probe["median_s"]
+    while count > 4096 and (steps + warmup) * t_call * (count / COUNT) > budget_s:
+        count //= 2
+    j = ref.time_collective("allreduce", "int32", count, P_RANKS, iters=steps, warmup=warmup, timeout=900)
+    if not j.get("ok"):
+        return {"error": "reference run failed", "detail": j}
+    t = j["median_s"]
+    gbs = 2 * P_RANKS * count * ES / t / 1e9
+    sample = (f"P=256 allreduce, {count} int32 per rank ({'full workload' if count == COUNT else 'scaled sample'}), "
+              f"{steps} timed calls after {warmup} warm-ups; per call: two barriers, wall time around one call, "
+              f"max over ranks, median over calls (bench/bench.cc:289-318, 376-387)")
+    return {"value": gbs, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference", "sample": sample,
+            "median_s": t, "count": count}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    r = reference_time(args.steps, max(args.warmup, 1))
+    if r is None or "error" in r:
+        why = "oracle/_ref/bine_ref_run is not built" if r is None else json.dumps(r)[:300]
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["median_s"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "P": P_RANKS, "count_per_rank": r["count"], "variant": "B", "ports": 1,
+                   "layer": "MPI (shim, one process per rank)"},
+        "cpu_baseline": {"value": r["value"], "unit": "GB/s", "cores": r["cores"], "kind": "reference",
+                         "sample": r["sample"]},
+        "e2e": {"value": r["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_engine_arm(args):
+    import numpy as np
+    import torch
+
+    import bine_trees_fugaku_b200 as bine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # Inputs: uniform int32 in [-1000, 1000] (or N(0,1) float32), one
+    # seeded stream per rank.
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(12345 + rank)
+    if args.dtype == "int32":
+        send = torch.randint(-1000, 1001, (P_RANKS, COUNT), dtype=torch.int32, device="cuda", generator=gen)
+        code = bine.INT32
+    else:
+        send = torch.randn((P_RANKS, COUNT), dtype=torch.float32, device="cuda", generator=gen)
+        code = bine.FLOAT
+    recv = torch.empty_like(send)
+    stream = torch.cuda.current_stream()
+    comm = bine.Comm(P_RANKS)
+    comm.set_stream(stream)
+    comm.set_algo("allreduce", "B")
+    comm.set_engine(args.engine)
+    comm.set_float_order(args.order)
+
+    def step():
+        comm.allreduce(send, recv, COUNT, code)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    comm.synchronize()
+    # Correctness of the timed configuration: exact integer sums; float
+    # sums within 1e-4 relative of FP64 (checked bit for bit by the tests).
+    if args.dtype == "int32":
+        expect = send.sum(0, dtype=torch.int64).to(torch.int32)
+        ok = bool(torch.equal(recv[0], expect) and torch.equal(recv[-1], expect))
+    else:
+        expect = send.double().sum(0)
+        ok = bool(torch.allclose(recv[0].double(), expect, rtol=1e-4, atol=1e-4) and torch.equal(recv[0], recv[-1]))
+        expect = recv[0].clone()
+
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        barrier()
+    elapsed_ms = start.elapsed_time(end)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = world * ALGO_BYTES / (ms_per_step * 1e-3) / 1e9
+    per_launch_gbs = ALGO_BYTES / (ms_per_step * 1e-3) / 1e9
+
+    # End to end through the C ABI with host buffers: each step copies the
+    # inputs from pinned host memory, runs the allreduce and reads every
+    # rank's result back.
+    host_in = torch.empty((P_RANKS, COUNT), dtype=send.dtype, pin_memory=True)
+    host_in.copy_(send.cpu())
+    host_out = torch.empty_like(host_in, pin_memory=True)
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 10))
+    for _ in range(2):
+        send.copy_(host_in, non_blocking=True)
+        step()
+        host_out.copy_(recv, non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        send.copy_(host_in, non_blocking=True)
+        step()
+        host_out.copy_(recv, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / max(1, e2e_steps)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    if e2e_steps:
+        ok = ok and bool(torch.equal(host_out[3], expect.cpu()))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = reference_time(10, 3, budget_s=60.0)
+        if r and "error" not in r:
+            cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    peak, peak_kind = peaks()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "P": P_RANKS, "count_per_rank": COUNT, "variant": "B", "ports": 1,
+                       "engine": "fused", "parallelism": f"replicas{world}",
+                       "l2": "inputs 1 GiB and outputs 1 GiB exceed the 126 MB L2; no flush"},
+            "roofline": {"bound": "hbm", "achieved": per_launch_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": per_launch_gbs / peak, "traffic": profiled_traffic(),
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "algorithmic_bytes_per_launch": ALGO_BYTES},
+            "cpu_baseline": cpu,
+            "e2e": None if not e2e_steps else {
+                "value": ALGO_BYTES / (e2e_ms * 1e-3) / 1e9 * world, "unit": "GB/s",
+                "h2d_bytes_per_step": P_RANKS * COUNT * ES, "d2h_bytes_per_step": P_RANKS * COUNT * ES,
+                "path": "Comm.allreduce (C ABI bine_allreduce) with pinned host buffers; every step copies all "
+                        "inputs to the GPU and every rank's result back"},
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+            "correct": ok,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    comm.close()
+    return 0 if ok else 1
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    # Profiling overrides; the defaults are the benchmark workload.
+    ap.add_argument("--P", type=int, default=256)
+    ap.add_argument("--count", type=int, default=1 << 20)
+    ap.add_argument("--dtype", default="int32", choices=["int32", "float"])
+    ap.add_argument("--engine", default="fused", choices=["fused", "steps"])
+    ap.add_argument("--order", default="reference", choices=["reference", "fast"])
+    args = ap.parse_args()
+    configure(args)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_engine_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

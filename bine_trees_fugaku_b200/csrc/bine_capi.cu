@@ -199,6 +199,15 @@ int get_dev_steps(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSt
         *out = it->second;
         return BINE_SUCCESS;
     }
+    // Every region the kernel will touch must lie inside its row: a planner
+    // error must never become an out-of-bounds device access.
+    const int64_t rows[3] = {s->send_elems, s->recv_elems, s->tmp_elems};
+    for (const auto& lvl : s->levels)
+        for (const Move& m : lvl)
+            for (const Region* r : {&m.dst, &m.a, &m.b})
+                if (r->rank < 0 || r->rank >= c->P || r->buf > kBufTmp || r->off < 0 || m.n < 0 ||
+                    r->off + m.n > rows[r->buf])
+                    return fail(BINE_ERR_INTERNAL, "planner produced a region outside its buffer row");
     auto d = std::make_shared<DevSteps>();
     std::vector<dev::StepMove> moves;
     std::vector<dev::StepChunk> chunks;
@@ -255,6 +264,17 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
     std::string err;
     if (!c->planner->trees(k, *s, &tp, &err)) return fail(BINE_ERR_INTERNAL, err);
     if (tp.max_depth > dev::kMaxTreeDepth) return fail(BINE_ERR_UNSUPPORTED, "reduction tree deeper than supported");
+    // Bounds of every leaf read and every output write, checked on the host.
+    for (const OutSegment& sg : tp.segs) {
+        if (sg.off < 0 || sg.n < 0 || sg.off + sg.n > s->recv_elems || sg.rank >= c->P ||
+            sg.prog_begin < 0 || sg.prog_begin + sg.prog_len > (int64_t)tp.prog.size())
+            return fail(BINE_ERR_INTERNAL, "reduction segment outside its buffer row");
+        for (int i = sg.prog_begin; i < sg.prog_begin + sg.prog_len; i++) {
+            const ProgEntry& e = tp.prog[i];
+            if (e.rank < 0 || e.rank >= c->P || sg.off + e.shift < 0 || sg.off + sg.n + e.shift > s->send_elems)
+                return fail(BINE_ERR_INTERNAL, "reduction leaf outside its input row");
+        }
+    }
     auto d = std::make_shared<DevTrees>();
     std::vector<dev::TreeSeg> segs;
     std::vector<dev::TreeEntry> prog;

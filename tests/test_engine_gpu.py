@@ -1,0 +1,229 @@
+"""GPU parity of the engine, through the C ABI, against the reference.
+
+* Every golden case (outputs of the reference library itself) is run on the
+  FUSED and on the STEPS engine and compared bit for bit, float32 included.
+* Larger cases are compared with the oracle (the C++ restatement).
+* Full-size properties (P = 256, 4 MiB per rank) use exact integer sums and
+  the FP64 tolerance of the reordered float path.
+Bit-exactness excludes NaN payloads (no input here produces NaNs).
+"""
+import numpy as np
+import pytest
+import torch
+
+import bine_trees_fugaku_b200 as bine
+from golden_data import load_ref_collectives
+from oracle import port
+from oracle.common import buffer_counts, expected, receiving_ranks
+from tests.golden.cases import case_input
+
+pytestmark = pytest.mark.gpu
+
+CASES = load_ref_collectives()
+NP2CODE = {np.dtype(np.int32): bine.INT32, np.dtype(np.int64): bine.INT64, np.dtype(np.float32): bine.FLOAT,
+           np.dtype(np.float64): bine.DOUBLE, np.dtype(np.int8): bine.CHAR}
+
+
+def make_comm(P, coll, variant, dims=None, ports=1, family="BINE", distance=None, engine="fused", order="reference"):
+    comm = bine.Comm(P, dims)
+    comm.set_ports(ports)
+    comm.set_algo(coll, variant, family, distance)
+    comm.set_engine(engine)
+    comm.set_float_order(order)
+    comm.set_stream(torch.cuda.current_stream())
+    return comm
+
+
+def run(comm, coll, x, count, root=0):
+    P = x.shape[0]
+    _, rc = buffer_counts(coll, count, P)
+    send = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    recv = torch.zeros((P, rc), dtype=send.dtype, device="cuda")
+    if coll == "bcast":
+        recv[root] = send[root]
+    comm.run(coll, send, recv, count, NP2CODE[x.dtype], root)
+    comm.synchronize()
+    return recv.cpu().numpy()
+
+
+def case_id(c):
+    return (f"{c['coll']}-{c['variant']}-P{c['P']}-{c['dtype']}-d{c.get('dims')}-p{c.get('ports', 1)}"
+            f"-r{c.get('root', 0)}-{c.get('family', 'BINE')}")
+
+
+@pytest.mark.parametrize("engine", ["fused", "steps"])
+@pytest.mark.parametrize("case", CASES, ids=case_id)
+def test_engine_matches_reference(case, engine):
+    x = case_input(case)
+    root = case.get("root", 0)
+    comm = make_comm(case["P"], case["coll"], case["variant"], case.get("dims"), case.get("ports", 1),
+                     case.get("family", "BINE"), case.get("distance"), engine)
+    rr = receiving_ranks(case["coll"], case["P"], root)
+    reduction = case["coll"] in ("allreduce", "reduce_scatter", "reduce")
+    try:
+        out = run(comm, case["coll"], x, case["count"], root)
+    except bine.Unsupported:
+        # Only cases the reference itself cannot run may be refused, and only
+        # by the engine that follows the reference's schedule or its exact
+        # float order.
+        assert engine == "steps" or (reduction and case["dtype"] == "float")
+        with pytest.raises(port.ReferenceUnsupported):
+            port.run(case["coll"], x, case["count"], variant=case["variant"], dims=case.get("dims"),
+                     ports=case.get("ports", 1), root=root, family=case.get("family", "BINE"),
+                     distance=case.get("distance"))
+        return
+    if case["ok"] and not _reference_ub(case, x):
+        assert np.array_equal(out[rr].view(np.uint8), case["out"][rr].view(np.uint8))
+    else:
+        # Reference-unsupported: MPI semantics (exact for integers and copies).
+        exp = expected(case["coll"], x, case["P"], case["count"], root)
+        assert np.array_equal(out[rr], exp[rr])
+
+
+def _reference_ub(case, x):
+    """Reference runs that only complete through undefined behaviour."""
+    try:
+        port.run(case["coll"], x, case["count"], variant=case["variant"], dims=case.get("dims"),
+                 ports=case.get("ports", 1), root=case.get("root", 0), family=case.get("family", "BINE"),
+                 distance=case.get("distance"))
+        return False
+    except port.ReferenceUnsupported:
+        return True
+
+
+@pytest.mark.parametrize("engine", ["fused", "steps"])
+@pytest.mark.parametrize("coll,variant,P,count,dims,ports", [
+    ("allreduce", "B", 64, 64 * 1000 + 13, None, 1),
+    ("allreduce", "B", 96, 96 * 512, None, 1),
+    ("allreduce", "B_COALESCE", 48, 48 * 777, None, 2),
+    ("allreduce", "B_CONT", 128, 128 * 256, None, 1),
+    ("allreduce", "L", 64, 50_000, None, 1),
+    ("allreduce", "L", 72, 30_000, [6, 12], 2),
+    ("allreduce", "B", 64, 64 * 600, [4, 4, 4], 6),
+    ("reduce_scatter", "VEC_HALVING_CONT_PERMUTE", 64, 1024, None, 1),
+    ("reduce", "BINOMIAL_TREE", 64, 20_000, None, 1),
+    ("reduce", "REDUCE_SCATTER_GATHER", 32, 20_001, None, 1),
+])
+def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
+    sc, _ = buffer_counts(coll, count, P)
+    x = np.random.default_rng(P + count).standard_normal((P, sc)).astype(np.float32)
+    expect, _ = port.run(coll, x, count, variant=variant, dims=dims, ports=ports)
+    comm = make_comm(P, coll, variant, dims, ports, engine=engine)
+    out = run(comm, coll, x, count)
+    rr = receiving_ranks(coll, P)
+    assert np.array_equal(out[rr].view(np.uint32), expect[rr].view(np.uint32))
+
+
+@pytest.mark.parametrize("coll", ["allgather", "bcast", "alltoall", "scatter", "gather"])
+@pytest.mark.parametrize("P,count,dt", [(64, 4096, np.float32), (32, 1001, np.int64), (16, 37, np.int8),
+                                        (256, 1024, np.int32)])
+def test_copies_large(coll, P, count, dt):
+    sc, _ = buffer_counts(coll, count, P)
+    x = (np.random.default_rng(P).standard_normal((P, sc)) * 100).astype(dt)
+    root = 3 % P
+    comm = make_comm(P, coll, list(bine.VARIANTS[coll])[0])
+    out = run(comm, coll, x, count, root)
+    rr = receiving_ranks(coll, P, root)
+    assert np.array_equal(out[rr], expected(coll, x, P, count, root)[rr])
+
+
+def test_full_size_int32_allreduce_is_exact():
+    """P = 256 virtual ranks, 4 MiB of int32 each (the benchmark workload)."""
+    P, count = 256, 1 << 20
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    send = torch.randint(-1000, 1001, (P, count), dtype=torch.int32, device="cuda", generator=g)
+    recv = torch.empty_like(send)
+    comm = make_comm(P, "allreduce", "B")
+    comm.allreduce(send, recv, count, bine.INT32)
+    comm.synchronize()
+    expect = send.sum(0, dtype=torch.int64).to(torch.int32)
+    assert torch.equal(recv, expect.expand(P, count))
+
+
+@pytest.mark.parametrize("P,count", [(256, 1 << 18), (1024, 1 << 14)])
+def test_full_size_int32_allreduce_steps_engine(P, count):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(2)
+    send = torch.randint(-1000, 1001, (P, count), dtype=torch.int32, device="cuda", generator=g)
+    recv = torch.empty_like(send)
+    comm = make_comm(P, "allreduce", "B", engine="steps")
+    comm.allreduce(send, recv, count, bine.INT32)
+    comm.synchronize()
+    assert torch.equal(recv, send.sum(0, dtype=torch.int64).to(torch.int32).expand(P, count))
+
+
+def test_fast_float_order_within_1e6_of_fp64():
+    """Reordered float32 path: |y - y64| <= 1e-6 |y64| elementwise, y64 the FP64 sum."""
+    P, count = 256, 1 << 20
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    send = torch.randn((P, count), dtype=torch.float32, device="cuda", generator=g)
+    recv = torch.empty_like(send)
+    comm = make_comm(P, "allreduce", "B", order="fast")
+    comm.allreduce(send, recv, count, bine.FLOAT)
+    comm.synchronize()
+    y64 = send.double().sum(0)
+    err = (recv[0].double() - y64).abs()
+    assert bool((err <= 1e-6 * y64.abs() + 1e-30).all())
+    assert torch.equal(recv[0], recv[-1])
+
+
+def test_full_size_float_reference_order_matches_oracle_columns():
+    """P = 256, 4 MiB float32 per rank in the reference order; sampled
+    columns are checked against the oracle run on the same columns' blocks."""
+    P, count = 256, 1 << 20
+    x = np.random.default_rng(4).standard_normal((P, count)).astype(np.float32)
+    comm = make_comm(P, "allreduce", "B")
+    send = torch.from_numpy(x).cuda()
+    recv = torch.empty_like(send)
+    comm.allreduce(send, recv, count, bine.FLOAT)
+    comm.synchronize()
+    got = recv[0].cpu().numpy()
+    # The reference's block b of rank r covers the same columns for every
+    # count that is a multiple of P: run the oracle on 4 columns per block.
+    blk = count // P
+    cols = np.concatenate([b * blk + np.array([0, 1, blk // 2, blk - 1]) for b in range(P)])
+    small = x[:, cols]
+    expect, _ = port.run("allreduce", small, small.shape[1], variant="B")
+    assert np.array_equal(got[cols].view(np.uint32), expect[0].view(np.uint32))
+    assert torch.equal(recv[0], recv[P - 1])
+
+
+def test_in_place_and_strided_layouts():
+    P, count = 32, 4099  # odd count: element-wise tail path
+    x = np.random.default_rng(5).integers(-1000, 1001, (P, count)).astype(np.int32)
+    comm = make_comm(P, "allreduce", "B")
+    buf = torch.from_numpy(x).cuda()
+    comm.allreduce(buf, buf, count, bine.INT32)  # MPI_IN_PLACE
+    comm.synchronize()
+    assert np.array_equal(buf.cpu().numpy(), expected("allreduce", x, P, count))
+    stride = 8192 * 4
+    big = torch.zeros((P, 8192), dtype=torch.int32, device="cuda")
+    big[:, :count] = torch.from_numpy(x).cuda()
+    out = torch.zeros_like(big)
+    comm.set_layout(stride, stride)
+    comm.allreduce(big, out, count, bine.INT32)
+    comm.synchronize()
+    assert np.array_equal(out[:, :count].cpu().numpy(), expected("allreduce", x, P, count))
+    assert int(out[:, count:].abs().sum()) == 0
+
+
+def test_step_engine_barrier_timeout_is_reported_and_recoverable():
+    """A grid barrier that can never open (fault injected on the host: it
+    waits for one arrival too many) expires after the configured bound; the
+    engine reports BINE_ERR_TIMEOUT and the next call works."""
+    P, count = 16, 16 * 64
+    x = np.random.default_rng(6).integers(-1000, 1001, (P, count)).astype(np.int32)
+    comm = make_comm(P, "allreduce", "B", engine="steps")
+    comm.set_step_timeout(200)
+    comm.debug_set_barrier_extra(1)
+    send = torch.from_numpy(x).cuda()
+    recv = torch.zeros_like(send)
+    comm.allreduce(send, recv, count, bine.INT32)
+    with pytest.raises(bine.Timeout):
+        comm.synchronize()
+    comm.debug_set_barrier_extra(0)
+    comm.allreduce(send, recv, count, bine.INT32)
+    comm.synchronize()
+    assert np.array_equal(recv.cpu().numpy(), expected("allreduce", x, P, count))
