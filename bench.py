@@ -179,6 +179,17 @@ def run_reference_arm(args):
     return 0
 
 
+def max_over_ranks(value, dist, device):
+    """Max of a per-rank float over all ranks (the slowest replica's time)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_engine_arm(args):
     import numpy as np
     import torch
@@ -246,11 +257,7 @@ def run_engine_arm(args):
             step()
         end.record(stream)
         barrier()
-    elapsed_ms = start.elapsed_time(end)
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(start.elapsed_time(end), dist, "cuda")
     ms_per_step = elapsed_ms / args.steps
     value = world * ALGO_BYTES / (ms_per_step * 1e-3) / 1e9
     per_launch_gbs = ALGO_BYTES / (ms_per_step * 1e-3) / 1e9
@@ -275,11 +282,7 @@ def run_engine_arm(args):
         host_out.copy_(recv, non_blocking=True)
     e1.record(stream)
     barrier()
-    e2e_ms = e0.elapsed_time(e1) / max(1, e2e_steps)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / max(1, e2e_steps), dist, "cuda")
     if e2e_steps:
         ok = ok and bool(torch.equal(host_out[3], expect.cpu()))
 

@@ -92,6 +92,8 @@ def lib():
         "bine_gather": [vp, i, i, vp, i, i, i, vp],
         "bine_reduce": [vp, vp, i, i, i, i, vp],
         "bine_plan_stats": [vp, i, ctypes.c_long, i, i64p],
+        "bine_plan_verify": [vp, i, ctypes.c_long, i],
+        "bine_link_bytes": [vp, i, ctypes.c_long, i, i, vp],
         "bine_plan_moves": [vp, i, ctypes.c_long, i, i64p, i64p, sz, ctypes.POINTER(sz)],
         "bine_plan_messages": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz)],
         "bine_plan_trees": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz)],
@@ -246,6 +248,15 @@ class Comm:
         out = (ctypes.c_int64 * 5)()
         check(lib().bine_plan_stats(self._h, COLL_ID[coll], count, root, out))
         return dict(zip(["levels", "moves", "messages", "tmp_elems", "traffic_elems"], list(out)))
+
+    def plan_verify(self, coll, count, root=0):
+        """Raises Unsupported when the reference's schedule is wrong here."""
+        check(lib().bine_plan_verify(self._h, COLL_ID[coll], count, root))
+
+    def link_bytes(self, coll, count, datatype, out, root=0):
+        """Per-link byte counts computed on the GPU into `out` (a CUDA
+        uint64/int64 tensor of 2*ndims*P entries)."""
+        check(lib().bine_link_bytes(self._h, COLL_ID[coll], count, datatype, root, _ptr(out)))
 
     def plan_moves(self, coll, count, root=0):
         n = ctypes.c_size_t(0)

@@ -199,6 +199,11 @@ int get_dev_steps(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSt
         *out = it->second;
         return BINE_SUCCESS;
     }
+    // The STEPS engine only runs schedules proven to compute the MPI result.
+    {
+        std::string verr;
+        if (!c->planner->verify(k, *s, &verr)) return fail(BINE_ERR_UNSUPPORTED, verr);
+    }
     // Every region the kernel will touch must lie inside its row: a planner
     // error must never become an out-of-bounds device access.
     const int64_t rows[3] = {s->send_elems, s->recv_elems, s->tmp_elems};
@@ -315,6 +320,15 @@ unsigned grid_for(const bine_comm_t c, long long work_items) {
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
 // ---------------------------------------------------------- fused kernels
+// Blocks of `kern` that fit on the device at once (resident capacity).
+template <typename K>
+unsigned resident_blocks(bine_comm_t c, K kern, int threads, size_t smem) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return (unsigned)(per_sm * std::max(1, c->num_sms));
+}
+
 template <typename T>
 int launch_sum(bine_comm_t c, int mode, const char* in, long long ist, char* out, long long ost, long long elems,
                long long blk, int root) {
@@ -326,7 +340,9 @@ int launch_sum(bine_comm_t c, int mode, const char* in, long long ist, char* out
     if (vec) {
         const long long ncol = elems * es / 16;
         if (ncol > 0) {
-            unsigned g = grid_for(c, ncol);
+            const long long tiles = (ncol + dev::kSumCols - 1) / dev::kSumCols;
+            const unsigned g = (unsigned)std::min<long long>(
+                tiles, resident_blocks(c, dev::k_sum_vec<T, dev::kSumAllreduce>, dev::kThreads, 0));
             const long long blk_vec = mode == dev::kSumReduceScatter ? blk * es / 16 : 0;
             if (mode == dev::kSumAllreduce)
                 dev::k_sum_vec<T, dev::kSumAllreduce><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol, blk_vec, root);
@@ -710,6 +726,15 @@ int bine_comm_synchronize(bine_comm_t comm) {
     return BINE_SUCCESS;
 }
 
+int bine_plan_verify(bine_comm_t comm, bine_coll_t coll, long count, int root) {
+    std::shared_ptr<Schedule> s;
+    int rc = plan_for_query(comm, coll, count, root, &s);
+    if (rc) return rc;
+    std::string err;
+    if (!comm->planner->verify(make_key(comm, coll, count, root), *s, &err)) return fail(BINE_ERR_UNSUPPORTED, err);
+    return BINE_SUCCESS;
+}
+
 int bine_plan_stats(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t out[5]) {
     std::shared_ptr<Schedule> s;
     int rc = plan_for_query(comm, coll, count, root, &s);
@@ -786,6 +811,69 @@ int bine_plan_trees(bine_comm_t comm, bine_coll_t coll, long count, int root, in
     }
     if (n_prog) *n_prog = tp.prog.size();
     if (n_segs) *n_segs = tp.segs.size();
+    return BINE_SUCCESS;
+}
+
+int bine_link_bytes(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                    uint64_t* d_link_bytes) {
+    if (!comm || !d_link_bytes) return fail(BINE_ERR_ARG, "null argument");
+    if ((int)coll < 0 || (int)coll >= kNumColls) return fail(BINE_ERR_ARG, "invalid collective");
+    if (count <= 0) return fail(BINE_ERR_ARG, "count must be positive");
+    const int es = dtype_size(datatype);
+    if (es < 0) return fail(BINE_ERR_ARG, "invalid datatype");
+    int rc = ensure_device(comm);
+    if (rc) return rc;
+    const Torus& t = comm->planner->torus();
+    const size_t nlinks = (size_t)t.size * t.ndims * 2;
+    unsigned long long* links = (unsigned long long*)d_link_bytes;
+    CUDA_TRY(cudaMemsetAsync(links, 0, nlinks * sizeof(unsigned long long), comm->stream));
+    bool all_p2 = true;
+    for (int d = 0; d < t.ndims; d++) all_p2 &= is_pow2(t.dims[d]);
+    const CollCfg& cf = comm->cfg[coll];
+    bool mirrored = false;
+    for (int p = 0; p < comm->ports; p++) mirrored |= mirrored_port(p, t.ndims);
+    int kind = -1;
+    if (all_p2 && (cf.family == kFamilyBine || !mirrored)) {
+        if (coll == kAllreduce && (cf.variant == kArB || cf.variant == kArBCoalesce) && cf.distance == kIncreasing &&
+            count >= (long)comm->ports * t.size)
+            kind = 0;
+        else if (coll == kAllreduce && cf.variant == kArL)
+            kind = 1;
+        else if (coll == kAllgather && cf.variant == kAgContPermute && cf.distance == kDecreasing)
+            kind = 2;
+    }
+    if (kind >= 0) {
+        dev::LinkGen g{t, cf.family, comm->ports, kind, (long long)count, es};
+        const long long threads = (long long)t.size * comm->ports;
+        unsigned grid = (unsigned)std::max(1LL, std::min((threads + 127) / 128, (long long)comm->num_sms * 32));
+        dev::k_link_generate<<<grid, 128, 0, comm->stream>>>(g, links);
+    } else {
+        std::shared_ptr<Schedule> s;
+        rc = plan_for_query(comm, coll, count, root, &s);
+        if (rc) return rc;
+        std::vector<long long> m(4 * s->messages.size());
+        for (size_t i = 0; i < s->messages.size(); i++) {
+            m[4 * i] = s->messages[i].level;
+            m[4 * i + 1] = s->messages[i].src;
+            m[4 * i + 2] = s->messages[i].dst;
+            m[4 * i + 3] = s->messages[i].elems;
+        }
+        if (!m.empty()) {
+            rc = ensure_work(comm, m.size() * sizeof(long long));
+            if (rc) return rc;
+            CUDA_TRY(cudaMemcpyAsync(comm->work, m.data(), m.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                                     comm->stream));
+            CUDA_TRY(cudaStreamSynchronize(comm->stream));  // m is a host temporary
+            const long long n = (long long)s->messages.size();
+            unsigned grid = (unsigned)std::max(1LL, std::min((n + 255) / 256, (long long)comm->num_sms * 16));
+            dev::k_link_from_msgs<<<grid, 256, 0, comm->stream>>>(t, (const long long*)comm->work, n, es, links);
+        }
+    }
+    long long nlines = 0;
+    for (int d = 0; d < t.ndims; d++) nlines += 2ll * (t.size / t.dims[d]);
+    unsigned grid = (unsigned)std::max(1LL, std::min((nlines + 127) / 128, (long long)comm->num_sms * 8));
+    dev::k_link_scan<<<grid, 128, 0, comm->stream>>>(t, links);
+    CUDA_TRY(cudaGetLastError());
     return BINE_SUCCESS;
 }
 

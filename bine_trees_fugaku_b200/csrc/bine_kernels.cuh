@@ -116,37 +116,70 @@ __device__ __forceinline__ uint4 vadd(uint4 a, uint4 b) {
 // ------------------------------------------------------- fused reductions
 enum SumMode { kSumAllreduce = 0, kSumReduceScatter = 1, kSumReduce = 2 };
 
-// Column sums over 16-byte vector columns.  `ncol` vector columns per input
-// row; reduce_scatter: `blk` vector columns per destination rank.
+// Column sums over 16-byte vector columns.  A block owns tiles of
+// kSumCols vector columns at a time; its 8 warps split the P rows of a
+// tile (warp g sums rows [g*P/8, (g+1)*P/8) of its lane's column, 8 loads in
+// flight per thread), the partial sums meet in shared memory, and all 256
+// threads then store the result rows.  Tiles are small (kSumCols * P * 16
+// bytes of input) and handed out grid-stride, so the load balances across
+// the 148 SMs with no wave tail.  `ncol` vector columns per input row;
+// reduce_scatter: `blk` vector columns per destination rank.
+constexpr int kSumCols = 32;
+constexpr int kSumGroups = kThreads / kSumCols;
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(kThreads) k_sum_vec(const char* __restrict__ in, long long in_stride,
                                                       char* __restrict__ out, long long out_stride, int P,
                                                       long long ncol, long long blk, int root) {
     using A = typename AccOf<T>::type;
-    const long long step = (long long)gridDim.x * blockDim.x;
-    for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += step) {
+    __shared__ Lanes<T, A> part[kSumGroups][kSumCols];
+    __shared__ uint4 res[kSumCols];
+    const int lane = threadIdx.x % kSumCols, grp = threadIdx.x / kSumCols;
+    const int per = (P + kSumGroups - 1) / kSumGroups;
+    const int r0 = min(P, grp * per), r1 = min(P, r0 + per);
+    const long long ntiles = (ncol + kSumCols - 1) / kSumCols;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long col = tile * kSumCols + lane;
         Lanes<T, A> acc;
         acc.zero();
-        const char* p = in + col * 16;
-        int r = 0;
-        for (; r + 8 <= P; r += 8) {
-            uint4 v[8];
+        if (col < ncol) {
+            const char* p = in + col * 16;
+            int r = r0;
+            for (; r + 8 <= r1; r += 8) {
+                uint4 v[8];
 #pragma unroll
-            for (int u = 0; u < 8; u++) v[u] = ld_stream(p + (long long)(r + u) * in_stride);
+                for (int u = 0; u < 8; u++) v[u] = ld_stream(p + (long long)(r + u) * in_stride);
 #pragma unroll
-            for (int u = 0; u < 8; u++) acc.add(v[u]);
+                for (int u = 0; u < 8; u++) acc.add(v[u]);
+            }
+            for (; r < r1; r++) acc.add(ld_stream(p + (long long)r * in_stride));
         }
-        for (; r < P; r++) acc.add(ld_stream(p + (long long)r * in_stride));
-        const uint4 res = acc.pack();
-        if (MODE == kSumAllreduce) {
-            char* q = out + col * 16;
-            for (int d = 0; d < P; d++) st_stream(q + (long long)d * out_stride, res);
-        } else if (MODE == kSumReduceScatter) {
-            long long owner = col / blk;
-            st_stream(out + owner * out_stride + (col - owner * blk) * 16, res);
-        } else {
-            st_stream(out + (long long)root * out_stride + col * 16, res);
+        part[grp][lane] = acc;
+        __syncthreads();
+        if (grp == 0) {
+            Lanes<T, A> s = part[0][lane];
+#pragma unroll
+            for (int g = 1; g < kSumGroups; g++)
+#pragma unroll
+                for (int i = 0; i < Lanes<T, A>::N; i++) s.v[i] = add_exact<A>(s.v[i], part[g][lane].v[i]);
+            res[lane] = s.pack();
         }
+        __syncthreads();
+        if (col < ncol) {
+            const uint4 v = res[lane];
+            if (MODE == kSumAllreduce) {
+                char* q = out + col * 16;
+                for (int d = grp; d < P; d += kSumGroups) st_stream(q + (long long)d * out_stride, v);
+            } else if (grp == 0) {
+                if (MODE == kSumReduceScatter) {
+                    const long long owner = col / blk;
+                    st_stream(out + owner * out_stride + (col - owner * blk) * 16, v);
+                } else {
+                    st_stream(out + (long long)root * out_stride + col * 16, v);
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -471,6 +504,162 @@ __global__ void __launch_bounds__(kThreads) k_steps(StepBufs B, const StepMove* 
             run_chunk<T>(B, moves[ch.move], ch);
         }
         if (l + 1 < nlevels && !grid_barrier(bar, status, timeout_ns, expected)) return;
+    }
+}
+
+}  // namespace dev
+}  // namespace bine
+
+// ------------------------------------------------------ torus link bytes
+// Per-link byte accounting of a schedule on the communicator's torus.  A
+// message moves along one dimension only (Bine and recursive-doubling peers
+// differ in one coordinate) and takes the minimal ring route, the +
+// direction on ties.  Link (node, d, dir) has index (node*ndims + d)*2 + dir
+// (dir 0: +, 1: -).  Each message adds its bytes to a cyclic range of link
+// positions on one ring, recorded as two or three signed updates of a
+// difference array (unsigned wrap-around arithmetic, exact mod 2^64); one
+// prefix scan per ring then yields the counts.  Cost: O(messages + links)
+// instead of O(messages * hops).
+#include "bine_sched.h"
+
+namespace bine {
+namespace dev {
+
+__device__ __forceinline__ size_t link_index(const Torus& t, int node, int d, int dir) {
+    return ((size_t)node * t.ndims + d) * 2 + dir;
+}
+
+// Adds `bytes` to the links of the minimal route src -> dst.
+__device__ __forceinline__ void add_route(const Torus& t, int src, int dst, unsigned long long bytes,
+                                          unsigned long long* diff) {
+    if (src == dst || bytes == 0) return;
+    int a[kMaxDims] = {0, 0, 0}, b[kMaxDims] = {0, 0, 0};
+    t.coords(src, a);
+    t.coords(dst, b);
+    int d = -1;
+    for (int i = 0; i < t.ndims; i++)
+        if (a[i] != b[i]) d = i;
+    if (d < 0) return;
+    const int L = t.dims[d];
+    const int delta = pmod(b[d] - a[d], L);
+    int dir = 0, start = a[d], hops = delta;
+    if (L - delta < delta) {  // minus direction: positions a-h+1 .. a
+        dir = 1;
+        hops = L - delta;
+        start = pmod(a[d] - hops + 1, L);
+    }
+    int c[kMaxDims] = {a[0], a[1], a[2]};
+    auto at = [&](int pos) {
+        c[d] = pos;
+        return link_index(t, t.id(c), d, dir);
+    };
+    const unsigned long long neg = 0ull - bytes;
+    const int end = start + hops;  // exclusive
+    atomicAdd(&diff[at(start)], bytes);
+    if (end < L) {
+        atomicAdd(&diff[at(end)], neg);
+    } else if (end > L) {  // wraps: [start, L) and [0, end - L)
+        atomicAdd(&diff[at(0)], bytes);
+        atomicAdd(&diff[at(end - L)], neg);
+    }
+}
+
+// One thread per message (src, dst, elements) of a host-planned schedule.
+__global__ void k_link_from_msgs(Torus t, const long long* __restrict__ msgs, long long n, int es,
+                                 unsigned long long* diff) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        add_route(t, (int)msgs[4 * i + 1], (int)msgs[4 * i + 2], (unsigned long long)msgs[4 * i + 3] * es, diff);
+}
+
+struct LinkGen {
+    Torus t;
+    int family, ports, kind;  // kind 0: bandwidth-optimal allreduce, 1: latency-optimal allreduce,
+                              //      2: contiguous allgather (distance halving)
+    long long count;          // the collective's count argument
+    int es;
+};
+
+// One thread per (rank, port): generates the messages of the schedule
+// directly from the step math (power-of-two torus dimensions only, where
+// every binomial tree visits each rank once).
+//   kind 0: the reduce-scatter message of rank r at step i carries the
+//   blocks of the subtree reached through peer_i(r) with later steps (the
+//   blocks whose block_step is i); the allgather sends the same volume back.
+//   kind 1: the full port slice to peer_i(r) at every step.
+//   kind 2: 2^s blocks to peer_{S-1-s}(r) at step s.
+__global__ void k_link_generate(LinkGen g, unsigned long long* diff) {
+    const long long total = (long long)g.t.size * g.ports;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(w / g.ports), port = (int)(w % g.ports);
+        StepDim sd[kMaxSteps];
+        step_dims(g.t, port, sd);
+        const int S = g.t.num_steps, P = g.t.size;
+        const long long cp = g.count / g.ports + (port < g.count % g.ports ? 1 : 0);
+        if (g.kind == 1) {
+            for (int i = 0; i < S; i++)
+                add_route(g.t, r, step_peer_rank(g.t, sd, i, port, g.family, r), (unsigned long long)cp * g.es, diff);
+            continue;
+        }
+        if (g.kind == 2) {
+            // Allgather blocks: by block, then port (count per block = count).
+            const long long b0 = g.count / g.ports + (port < g.count % g.ports ? 1 : 0);
+            for (int s = 0; s < S; s++)
+                add_route(g.t, r, step_peer_rank(g.t, sd, S - 1 - s, port, g.family, r),
+                          ((unsigned long long)1 << s) * b0 * g.es, diff);
+            continue;
+        }
+        const long long q = cp / P, rem = cp % P;
+        for (int i = 0; i < S; i++) {
+            const int child = step_peer_rank(g.t, sd, i, port, g.family, r);
+            // Iterative walk of child's subtree along steps > i.
+            int stk_node[kMaxSteps * (kMaxSteps + 1) / 2 + 1];
+            int8_t stk_step[kMaxSteps * (kMaxSteps + 1) / 2 + 1];
+            int sp = 0;
+            stk_node[sp] = child;
+            stk_step[sp++] = (int8_t)(i + 1);
+            unsigned long long elems = 0;
+            while (sp > 0) {
+                const int node = stk_node[--sp];
+                const int st = stk_step[sp];
+                elems += (unsigned long long)(q + (node < rem ? 1 : 0));
+                for (int j = st; j < S; j++) {
+                    stk_node[sp] = step_peer_rank(g.t, sd, j, port, g.family, node);
+                    stk_step[sp++] = (int8_t)(j + 1);
+                }
+            }
+            add_route(g.t, r, child, elems * g.es, diff);  // reduce-scatter step i
+            add_route(g.t, child, r, elems * g.es, diff);  // allgather step S-1-i
+        }
+    }
+}
+
+// One thread per ring: prefix sums of the difference array, in place.
+__global__ void k_link_scan(Torus t, unsigned long long* links) {
+    long long nlines = 0;
+    long long base[kMaxDims];
+    for (int d = 0; d < t.ndims; d++) {
+        base[d] = nlines;
+        nlines += 2ll * (t.size / t.dims[d]);
+    }
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < nlines; w += (long long)gridDim.x * blockDim.x) {
+        int d = 0;
+        while (d + 1 < t.ndims && w >= base[d + 1]) d++;
+        const long long k = w - base[d];
+        const int dir = (int)(k & 1);
+        long long line = k >> 1;  // index over the other coordinates
+        int c[kMaxDims] = {0, 0, 0};
+        for (int i = t.ndims - 1; i >= 0; i--) {
+            if (i == d) continue;
+            c[i] = (int)(line % t.dims[i]);
+            line /= t.dims[i];
+        }
+        unsigned long long acc = 0;
+        for (int p = 0; p < t.dims[d]; p++) {
+            c[d] = p;
+            const size_t li = link_index(t, t.id(c), d, dir);
+            acc += links[li];
+            links[li] = acc;
+        }
     }
 }
 

@@ -1537,6 +1537,86 @@ bool Planner::trees(const PlanKey& k, const Schedule& s, TreePlan* out, std::str
     return true;
 }
 
+bool Planner::verify(const PlanKey& k, const Schedule& s, std::string* err) const {
+    const int P = t_.size;
+    const int64_t c = k.count;
+    SymExec ex(P);
+    if (k.coll == kBcast) {
+        ex.set(ex.buf(k.root, kBufRecv), 0, s.recv_elems, Val{ex.leaf(k.root), 0});
+    } else {
+        for (int r = 0; r < P; r++) ex.set(ex.buf(r, kBufSend), 0, s.send_elems, Val{ex.leaf(r), 0});
+    }
+    for (const auto& lvl : s.levels)
+        for (const Move& m : lvl) ex.apply(m);
+    const bool reduction = k.coll == kAllreduce || k.coll == kReduceScatter || k.coll == kReduce;
+    std::vector<int> ranks;
+    if (k.coll == kReduce || k.coll == kGather) ranks.push_back(k.root);
+    else
+        for (int r = 0; r < P; r++) ranks.push_back(r);
+    // Expected source (rank, shift) of output element p on rank r.
+    auto expect = [&](int r, int64_t p, int* src, int64_t* shift) {
+        switch (k.coll) {
+        case kAllgather: *src = (int)(p / c); *shift = -(p / c) * c; break;
+        case kBcast: *src = k.root; *shift = 0; break;
+        case kAlltoall: *src = (int)(p / c); *shift = (int64_t)r * c - (p / c) * c; break;
+        case kScatter: *src = k.root; *shift = (int64_t)r * c; break;
+        case kGather: *src = (int)(p / c); *shift = -(p / c) * c; break;
+        case kReduceScatter: *src = -1; *shift = (int64_t)r * c; break;
+        default: *src = -1; *shift = 0; break;
+        }
+    };
+    std::map<std::pair<int32_t, int64_t>, bool> checked;  // reduction trees already proven
+    std::vector<char> seen;
+    std::function<bool(int32_t, int64_t, int64_t)> walk = [&](int32_t id, int64_t sh, int64_t want) -> bool {
+        const Node& n = ex.node(id);
+        if (n.left < 0) {
+            if (sh != want || seen[n.rank]) return false;
+            seen[n.rank] = 1;
+            return true;
+        }
+        return walk(n.left, sh, want) && walk(n.right, sh + n.rshift, want);
+    };
+    for (int r : ranks) {
+        auto runs = ex.get(ex.buf(r, kBufRecv), 0, s.recv_elems);
+        for (auto& t : runs) {
+            const int64_t lo = std::get<0>(t), hi = std::get<1>(t);
+            const Val v = std::get<2>(t);
+            if (v.node < 0) {
+                *err = "the reference's schedule leaves output elements unwritten here";
+                return false;
+            }
+            if (reduction) {
+                int src;
+                int64_t want;
+                expect(r, lo, &src, &want);
+                auto key = std::make_pair(v.node, v.shift - want);
+                if (checked.count(key)) continue;
+                seen.assign(P, 0);
+                if (ex.node(v.node).leaves != P || !walk(v.node, v.shift, want)) {
+                    *err = "the reference's schedule does not sum every rank exactly once here (wrong data)";
+                    return false;
+                }
+                checked[key] = true;
+                continue;
+            }
+            // Copies: one source block per output block of c elements.
+            for (int64_t p = lo; p < hi;) {
+                int src;
+                int64_t want;
+                expect(r, p, &src, &want);
+                const int64_t blk_end = (k.coll == kBcast || k.coll == kScatter) ? hi : std::min(hi, (p / c + 1) * c);
+                const Node& n = ex.node(v.node);
+                if (n.left >= 0 || n.rank != src || v.shift != want) {
+                    *err = "the reference's schedule delivers the wrong block here (wrong data)";
+                    return false;
+                }
+                p = blk_end;
+            }
+        }
+    }
+    return true;
+}
+
 bool link_bytes(const Torus& t, const std::vector<Message>& msgs, int es, std::vector<uint64_t>* out,
                 std::string* err) {
     out->assign((size_t)t.size * t.ndims * 2, 0);

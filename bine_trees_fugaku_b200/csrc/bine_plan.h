@@ -136,6 +136,13 @@ class Planner {
     // Exact reduction trees of every output element (float reference order).
     bool trees(const PlanKey& k, const Schedule& s, TreePlan* out, std::string* err) const;
 
+    // Proves, by symbolic execution, that the schedule computes the
+    // collective's MPI result: every output element is exactly the input
+    // element the MPI semantics name, or for reductions the sum of that
+    // element over every rank exactly once.  Returns false (with `err`)
+    // when the reference's schedule returns wrong data for this case.
+    bool verify(const PlanKey& k, const Schedule& s, std::string* err) const;
+
   private:
     Torus t_;
 };

@@ -175,6 +175,13 @@ int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
  * and need no GPU.  `count` and `root` have the meaning of the collective's
  * own arguments (for reduce_scatter, the per-rank receive count). */
 
+/* Proves by symbolic execution that the planned schedule computes the MPI
+ * result (every output element is the right input element, or the sum of
+ * that element over every rank once); BINE_ERR_UNSUPPORTED when the
+ * reference's schedule returns wrong data for this case.  The STEPS engine
+ * runs only verified schedules. */
+int bine_plan_verify(bine_comm_t comm, bine_coll_t coll, long count, int root);
+
 /* Sizes of the schedule: out[0] = steps (levels), out[1] = moves,
  * out[2] = messages, out[3] = workspace elements per rank,
  * out[4] = bytes read + written by the STEPS engine per element size. */
@@ -203,6 +210,18 @@ int bine_plan_trees(bine_comm_t comm, bine_coll_t coll, long count, int root, in
  * host from the planned schedule. */
 int bine_link_bytes_host(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
                          uint64_t *link_bytes, size_t cap);
+
+/* The same per-link byte counts computed on the GPU into the device array
+ * d_link_bytes (2*ndims*nranks uint64 values, overwritten), asynchronously
+ * on the communicator's stream.  For the bandwidth-optimal (B, B_COALESCE)
+ * and latency-optimal (L) allreduce and the contiguous allgather on tori
+ * whose dimensions are powers of two, the messages are generated on the
+ * device from the step math (no host planning, any size up to 2^20
+ * ranks); other cases aggregate the planned message list on the device.
+ * Stands in for the link traffic of simulation/simulator.py:125-177 and
+ * simulation/out_bytes.py:18-69. */
+int bine_link_bytes(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                    uint64_t *d_link_bytes);
 
 #ifdef __cplusplus
 }

@@ -102,3 +102,29 @@ def test_link_bytes_conserve_message_volume():
         expect += n * 4 * min(delta, d[k] - delta)
     assert int(lb.sum()) == expect
     assert lb.shape == (64 * 3 * 2,)
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["ok"]], ids=lambda c: f"{c['coll']}-{c['variant']}-P{c['P']}"
+                         f"-{c['dtype']}-d{c.get('dims')}-p{c.get('ports', 1)}-r{c.get('root', 0)}-{c.get('family', 'BINE')}")
+def test_verify_flags_exactly_the_wrong_reference_results(case):
+    """The planner's symbolic proof fails exactly where the reference
+    completes with data that is not the MPI result."""
+    from oracle.common import expected
+    x = case_input(case)
+    comm = make_comm(case)
+    root = case.get("root", 0)
+    try:
+        comm.plan_stats(case["coll"], case["count"], root)
+    except bine.Unsupported:
+        return  # not even plannable (undefined behaviour in the reference)
+    rr = receiving_ranks(case["coll"], case["P"], root)
+    exp = expected(case["coll"], x, case["P"], case["count"], root)
+    if case["dtype"] == "float" and case["coll"] in ("allreduce", "reduce_scatter", "reduce"):
+        right = np.allclose(case["out"][rr], exp[rr], rtol=1e-4, atol=1e-4)
+    else:
+        right = np.array_equal(case["out"][rr], exp[rr])
+    if right:
+        comm.plan_verify(case["coll"], case["count"], root)
+    else:
+        with pytest.raises(bine.Unsupported):
+            comm.plan_verify(case["coll"], case["count"], root)
