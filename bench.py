@@ -323,6 +323,150 @@ def run_engine_arm(args):
     return 0 if ok else 1
 
 
+def batch_workload(n=4096, seed=2024, budget_bytes=48 << 30):
+    """The batched workload: n independent collectives, P ~ U[4, 512], per-rank
+    message log-uniform from 64 B, op mix 50% allreduce / 25% reduce_scatter /
+    25% allgather, dtype mix float32 N(0,1) / int32 U[-1000, 1000].
+
+    The per-rank message is the larger per-rank buffer (allreduce send =
+    receive, reduce_scatter send, allgather receive); counts are rounded down
+    to whole 16-byte vectors (at least one).  Inputs are views of one shared,
+    read-only pool of 512 rows of 4 MiB; outputs are distinct.  The
+    log-uniform upper bound starts at 4 MiB and is halved until the outputs
+    fit `budget_bytes` (the stated sizes would need ~400 GB for the
+    allreduces alone); the bound used is reported."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    P = rng.integers(4, 513, n)
+    u = rng.random(n)
+    op = rng.choice(3, n, p=[0.5, 0.25, 0.25])
+    is_float = rng.random(n) < 0.5
+    upper = 4 << 20
+    while True:
+        m = np.exp(np.log(64) + u * (np.log(upper) - np.log(64)))
+        items, out_bytes = [], 0
+        for k in range(n):
+            p = int(P[k])
+            if op[k] == 0:
+                c = max(4, int(m[k] // 4) // 4 * 4)
+                ob = p * c * 4
+            else:
+                c = max(4, int(m[k] // (4 * p)) // 4 * 4)
+                ob = p * c * 4 * (p if op[k] == 2 else 1)
+            items.append((["allreduce", "reduce_scatter", "allgather"][op[k]], p, c, bool(is_float[k]), ob))
+            out_bytes += ob
+        if out_bytes <= budget_bytes or upper <= 1024:
+            return items, upper, out_bytes
+        upper //= 2
+
+
+def run_batch_suite(args):
+    import numpy as np
+    import torch
+
+    import bine_trees_fugaku_b200 as bine
+    from bine_trees_fugaku_b200 import tuning
+
+    torch.cuda.set_device(0)
+    spec, upper, out_bytes = batch_workload(args.batch_n)
+    pool_rows, pool_row = 512, 4 << 20
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    pool_i = torch.randint(-1000, 1001, (pool_rows, pool_row // 4), dtype=torch.int32, device="cuda", generator=g)
+    pool_f = torch.randn((pool_rows, pool_row // 4), dtype=torch.float32, device="cuda", generator=g)
+    outs, items, algo_bytes = [], [], 0
+    for coll, p, c, fl, ob in spec:
+        out = torch.empty(ob // 4, dtype=torch.float32 if fl else torch.int32, device="cuda")
+        outs.append(out)
+        send = (pool_f if fl else pool_i)
+        items.append((coll, send, out, c, bine.FLOAT if fl else bine.INT32, p, pool_row, 0))
+        if coll == "allreduce":
+            algo_bytes += 2 * p * c * 4
+        elif coll == "reduce_scatter":
+            algo_bytes += p * p * c * 4 + p * c * 4
+        else:
+            algo_bytes += p * c * 4 + p * p * c * 4
+    stream = torch.cuda.current_stream()
+    # Per-call baseline: one FUSED launch per collective (FAST float order).
+    comms = {}
+    for coll, send, out, c, dt, p, _, _ in items:
+        if p not in comms:
+            cm = bine.Comm(p)
+            cm.set_stream(stream)
+            cm.set_float_order("fast")
+            cm.set_layout(pool_row, 0)
+            comms[p] = cm
+
+    def per_call():
+        for coll, send, out, c, dt, p, _, _ in items:
+            comms[p].run(coll, send, out, c, dt)
+
+    per_call()
+    torch.cuda.synchronize()
+    ref_sums = torch.stack([o.view(torch.int32).to(torch.int64).sum() for o in outs])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = args.steps
+    e0.record(stream)
+    for _ in range(reps):
+        per_call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    per_call_ms = e0.elapsed_time(e1) / reps
+
+    # Autotuned batched launch (tuning cached on disk with a checksum).
+    cache = os.path.join(ROOT, "gpurun_out", "batch_tuning.json") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) \
+        else os.path.join(ROOT, ".batch_tuning.json")
+    table = tuning.load(cache)
+    sig = tuning.signature(items, torch.cuda.get_device_name(0))
+    tune_ms = None
+    if sig in table:
+        tu = bine.BatchTuning.from_dict(table[sig])
+    else:
+        tu, tune_ms = bine.Batch.autotune(items, stream, reps=2)
+        table[sig] = tu.as_dict()
+        tuning.save(cache, table)
+    batch = bine.Batch(items, tu)
+    for o in outs:
+        o.zero_()
+    batch.launch(stream)
+    torch.cuda.synchronize()
+    sums = torch.stack([o.view(torch.int32).to(torch.int64).sum() for o in outs])
+    fl = torch.tensor([it[4] == bine.FLOAT for it in items], device="cuda")
+    exact = bool(torch.equal(sums[~fl], ref_sums[~fl]))
+    # Captured in a CUDA graph: one graph launch per batch.
+    graph = torch.cuda.CUDAGraph()
+    s2 = torch.cuda.Stream()
+    s2.wait_stream(stream)
+    with torch.cuda.stream(s2):
+        with torch.cuda.graph(graph, stream=s2):
+            batch.launch(s2)
+    stream.wait_stream(s2)
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1) / reps
+    line = {"suite": "batch", "metric": "batched collectives throughput", "unit": "GB/s",
+            "value": algo_bytes / (batch_ms * 1e-3) / 1e9,
+            "per_call_value": algo_bytes / (per_call_ms * 1e-3) / 1e9,
+            "speedup_vs_one_launch_per_collective": per_call_ms / batch_ms,
+            "batch_ms": batch_ms, "per_call_ms": per_call_ms, "collectives": len(items),
+            "collectives_per_s": len(items) / (batch_ms * 1e-3),
+            "integer_results_equal_single_calls": exact,
+            "config": {"n": len(items), "P": "U[4,512]", "message": f"log-uniform [64 B, {upper} B] (per-rank, larger buffer)",
+                       "mix": "50% allreduce / 25% reduce_scatter / 25% allgather; float32 N(0,1) / int32 U[-1000,1000]",
+                       "output_bytes": out_bytes, "algorithmic_bytes": algo_bytes, "inputs": "shared read-only pool 512 x 4 MiB",
+                       "tuning": tu.as_dict(), "autotune_ms": tune_ms, "graph": "one CUDA graph replay per batch"}}
+    print(json.dumps(line))
+    batch.close()
+    return 0 if exact else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,8 +481,12 @@ def main():
     ap.add_argument("--dtype", default="int32", choices=["int32", "float"])
     ap.add_argument("--engine", default="fused", choices=["fused", "steps"])
     ap.add_argument("--order", default="reference", choices=["reference", "fast"])
+    ap.add_argument("--suite", default="headline", choices=["headline", "batch"])
+    ap.add_argument("--batch-n", type=int, default=4096)
     args = ap.parse_args()
     configure(args)
+    if args.suite == "batch":
+        return run_batch_suite(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

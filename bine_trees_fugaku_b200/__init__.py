@@ -43,6 +43,32 @@ DTYPE_SIZE = {INT32: 4, INT64: 8, FLOAT: 4, DOUBLE: 8, CHAR: 1}
 NP_DTYPE = {INT32: np.int32, INT64: np.int64, FLOAT: np.float32, DOUBLE: np.float64, CHAR: np.int8}
 
 
+class BatchItem(ctypes.Structure):
+    """bine_batch_item_t"""
+    _fields_ = [("coll", ctypes.c_int), ("datatype", ctypes.c_int), ("nranks", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("count", ctypes.c_long), ("sendbuf", ctypes.c_void_p),
+                ("recvbuf", ctypes.c_void_p), ("send_stride", ctypes.c_size_t), ("recv_stride", ctypes.c_size_t)]
+
+
+class BatchTuning(ctypes.Structure):
+    """bine_batch_tuning_t"""
+    _fields_ = [("rank_bound", ctypes.c_int * 4), ("tile_cols", ctypes.c_int * 4), ("grid_mult", ctypes.c_int),
+                ("order", ctypes.c_int)]
+
+    def as_dict(self):
+        return {"rank_bound": list(self.rank_bound), "tile_cols": list(self.tile_cols),
+                "grid_mult": self.grid_mult, "order": self.order}
+
+    @classmethod
+    def from_dict(cls, d):
+        t = cls()
+        for k in range(4):
+            t.rank_bound[k] = d["rank_bound"][k]
+            t.tile_cols[k] = d["tile_cols"][k]
+        t.grid_mult, t.order = d["grid_mult"], d["order"]
+        return t
+
+
 class BineError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"bine error {code}: {msg}")
@@ -98,6 +124,11 @@ def lib():
         "bine_plan_messages": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz)],
         "bine_plan_trees": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz)],
         "bine_link_bytes_host": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(ctypes.c_uint64), sz],
+        "bine_batch_create": [ctypes.POINTER(BatchItem), i, ctypes.POINTER(BatchTuning), ctypes.POINTER(vp)],
+        "bine_batch_launch": [vp, vp],
+        "bine_batch_destroy": [vp],
+        "bine_batch_autotune": [ctypes.POINTER(BatchItem), i, vp, i, ctypes.POINTER(BatchTuning),
+                                ctypes.POINTER(ctypes.c_float)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -308,3 +339,55 @@ def row_counts(coll, count, P):
     if coll == "alltoall":
         return count * P, count * P
     raise ValueError(coll)
+
+
+class Batch:
+    """Many allreduce / reduce_scatter / allgather calls in one persistent
+    launch (bine_batch_*).  `items` are (coll, sendbuf, recvbuf, count,
+    datatype, nranks[, send_stride, recv_stride]) tuples of CUDA tensors
+    laid out (nranks, row); strides in bytes, 0 = packed rows."""
+
+    def __init__(self, items, tuning=None):
+        self._items = self.make_items(items)
+        self._h = ctypes.c_void_p()
+        tu = ctypes.byref(tuning) if tuning is not None else None
+        check(lib().bine_batch_create(self._items, len(items), tu, ctypes.byref(self._h)))
+
+    @staticmethod
+    def make_items(items):
+        arr = (BatchItem * max(1, len(items)))()
+        for k, it in enumerate(items):
+            coll, send, recv, count, dt, P = it[:6]
+            arr[k].send_stride = it[6] if len(it) > 6 else 0
+            arr[k].recv_stride = it[7] if len(it) > 7 else 0
+            arr[k].coll = COLL_ID[coll]
+            arr[k].datatype = dt
+            arr[k].nranks = P
+            arr[k].count = count
+            arr[k].sendbuf = _ptr(send)
+            arr[k].recvbuf = _ptr(recv)
+        return arr
+
+    def launch(self, stream=None):
+        h = stream if isinstance(stream, int) else (stream.cuda_stream if stream is not None else 0)
+        check(lib().bine_batch_launch(self._h, h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bine_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def autotune(items, stream=None, reps=3):
+        arr = Batch.make_items(items)
+        best = BatchTuning()
+        ms = ctypes.c_float()
+        h = stream if isinstance(stream, int) else (stream.cuda_stream if stream is not None else 0)
+        check(lib().bine_batch_autotune(arr, len(items), h, reps, ctypes.byref(best), ctypes.byref(ms)))
+        return best, ms.value

@@ -550,7 +550,190 @@ int plan_for_query(bine_comm_t c, int coll, long count, int root, std::shared_pt
 
 }  // namespace
 
+// ---------------------------------------------------------------- batches
+struct bine_batch_s {
+    dev::BatchItem* items = nullptr;
+    int nitems = 0;
+    long long total_tiles = 0;
+    unsigned grid = 1;
+    ~bine_batch_s() { cudaFree(items); }
+};
+
+namespace {
+
+const bine_batch_tuning_t kDefaultTuning = {{8, 32, 128, 1 << 30}, {256, 128, 64, 32}, 1, 1};
+
+int batch_layout(const bine_batch_item_t* items, int n, const bine_batch_tuning_t& tu,
+                 std::vector<dev::BatchItem>* out, long long* total_tiles) {
+    out->clear();
+    std::vector<std::pair<double, int>> order;
+    for (int i = 0; i < n; i++) {
+        const bine_batch_item_t& x = items[i];
+        if (x.coll != BINE_COLL_ALLREDUCE && x.coll != BINE_COLL_REDUCE_SCATTER && x.coll != BINE_COLL_ALLGATHER)
+            return fail(BINE_ERR_ARG, "batch item " + std::to_string(i) + ": only allreduce, reduce_scatter and allgather");
+        if (x.datatype != BINE_INT32 && x.datatype != BINE_FLOAT)
+            return fail(BINE_ERR_ARG, "batch item " + std::to_string(i) + ": datatype must be BINE_INT32 or BINE_FLOAT");
+        if (x.nranks < 1 || x.count < 1 || !x.sendbuf || !x.recvbuf)
+            return fail(BINE_ERR_ARG, "batch item " + std::to_string(i) + ": bad nranks, count or buffer");
+        if ((x.count * 4) % 16)
+            return fail(BINE_ERR_ARG, "batch item " + std::to_string(i) + ": count must fill whole 16-byte vectors");
+        const long long P = x.nranks, row = x.count * 4;
+        long long se = row, re = row;
+        if (x.coll == BINE_COLL_REDUCE_SCATTER) se = row * P;
+        if (x.coll == BINE_COLL_ALLGATHER) re = row * P;
+        dev::BatchItem b;
+        b.in = (const char*)x.sendbuf;
+        b.out = (char*)x.recvbuf;
+        b.in_stride = x.send_stride ? (long long)x.send_stride : se;
+        b.out_stride = x.recv_stride ? (long long)x.recv_stride : re;
+        if (b.in_stride < se || b.out_stride < re || (b.in_stride | b.out_stride) % 16 || !aligned16(b.in) || !aligned16(b.out))
+            return fail(BINE_ERR_ARG, "batch item " + std::to_string(i) + ": rows must be 16-byte aligned and fit their stride");
+        b.P = x.nranks;
+        b.is_float = x.datatype == BINE_FLOAT;
+        b.blk = 0;
+        double cost;
+        if (x.coll == BINE_COLL_ALLGATHER) {
+            b.op = dev::kBatchAllgather;
+            b.ncol = row / 16;
+            b.tc = dev::kThreads;
+            b.ntiles = (P * b.ncol + dev::kThreads - 1) / dev::kThreads;
+            cost = (double)P * b.ncol * (P + 1);
+        } else {
+            b.op = x.coll == BINE_COLL_ALLREDUCE ? dev::kBatchAllreduce : dev::kBatchReduceScatter;
+            b.ncol = se / 16;
+            b.blk = x.coll == BINE_COLL_REDUCE_SCATTER ? row / 16 : 0;
+            int tc = tu.tile_cols[3];
+            for (int k = 0; k < 4; k++)
+                if (x.nranks <= tu.rank_bound[k]) {
+                    tc = tu.tile_cols[k];
+                    break;
+                }
+            if (tc != 32 && tc != 64 && tc != 128 && tc != 256) return fail(BINE_ERR_ARG, "tile_cols must be 32, 64, 128 or 256");
+            b.tc = tc;
+            b.ntiles = (b.ncol + tc - 1) / tc;
+            cost = (double)P * b.ncol * (x.coll == BINE_COLL_ALLREDUCE ? 2 : 1);
+        }
+        out->push_back(b);
+        order.push_back({cost, i});
+    }
+    if (tu.order == 1) {
+        std::stable_sort(order.begin(), order.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+            return a.first > b.first;
+        });
+        std::vector<dev::BatchItem> sorted;
+        for (auto& o : order) sorted.push_back((*out)[o.second]);
+        *out = sorted;
+    }
+    long long t = 0;
+    for (auto& b : *out) {
+        b.tile_begin = t;
+        t += b.ntiles;
+    }
+    *total_tiles = t;
+    return BINE_SUCCESS;
+}
+
+unsigned batch_grid(long long total_tiles, int grid_mult) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_batch, dev::kThreads, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    long long g = (long long)per_sm * sms * std::max(1, grid_mult);
+    return (unsigned)std::max(1LL, std::min(g, total_tiles));
+}
+
+}  // namespace
+
 extern "C" {
+
+int bine_batch_create(const bine_batch_item_t* items, int nitems, const bine_batch_tuning_t* tuning,
+                      bine_batch_t* batch) {
+    if (!batch || (!items && nitems > 0) || nitems < 0) return fail(BINE_ERR_ARG, "bad batch arguments");
+    *batch = nullptr;
+    const bine_batch_tuning_t& tu = tuning ? *tuning : kDefaultTuning;
+    std::vector<dev::BatchItem> v;
+    long long tiles = 0;
+    int rc = batch_layout(items, nitems, tu, &v, &tiles);
+    if (rc) return rc;
+    auto b = std::unique_ptr<bine_batch_s>(new bine_batch_s());
+    b->nitems = (int)v.size();
+    b->total_tiles = tiles;
+    b->grid = batch_grid(tiles, tu.grid_mult);
+    if (!v.empty()) {
+        CUDA_TRY(cudaMalloc(&b->items, v.size() * sizeof(dev::BatchItem)));
+        CUDA_TRY(cudaMemcpy(b->items, v.data(), v.size() * sizeof(dev::BatchItem), cudaMemcpyHostToDevice));
+    }
+    *batch = b.release();
+    return BINE_SUCCESS;
+}
+
+int bine_batch_launch(bine_batch_t batch, void* stream) {
+    if (!batch) return fail(BINE_ERR_ARG, "null batch");
+    if (batch->total_tiles == 0) return BINE_SUCCESS;
+    dev::k_batch<<<batch->grid, dev::kThreads, 0, (cudaStream_t)stream>>>(batch->items, batch->nitems, batch->total_tiles);
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
+int bine_batch_destroy(bine_batch_t batch) {
+    delete batch;
+    return BINE_SUCCESS;
+}
+
+int bine_batch_autotune(const bine_batch_item_t* items, int nitems, void* stream, int reps, bine_batch_tuning_t* best,
+                        float* best_ms) {
+    if (!best || reps < 1) return fail(BINE_ERR_ARG, "bad autotune arguments");
+    // Candidate tile policies: (rank bound, tile columns) pairs.
+    const bine_batch_tuning_t policies[] = {
+        {{8, 32, 128, 1 << 30}, {256, 128, 64, 32}, 1, 0},
+        {{4, 16, 64, 1 << 30}, {256, 128, 64, 32}, 1, 0},
+        {{16, 64, 256, 1 << 30}, {256, 128, 64, 32}, 1, 0},
+        {{32, 128, 512, 1 << 30}, {128, 64, 64, 32}, 1, 0},
+        {{1 << 30, 1 << 30, 1 << 30, 1 << 30}, {32, 32, 32, 32}, 1, 0},
+        {{1 << 30, 1 << 30, 1 << 30, 1 << 30}, {64, 64, 64, 64}, 1, 0},
+    };
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best_t = 1e30f;
+    int rc = BINE_SUCCESS;
+    for (const auto& pol : policies) {
+        for (int gm : {1, 2, 4}) {
+            for (int order : {0, 1}) {
+                bine_batch_tuning_t tu = pol;
+                tu.grid_mult = gm;
+                tu.order = order;
+                bine_batch_t b = nullptr;
+                rc = bine_batch_create(items, nitems, &tu, &b);
+                if (rc) goto done;
+                bine_batch_launch(b, stream);  // warm-up
+                cudaEventRecord(e0, s);
+                for (int r = 0; r < reps; r++) bine_batch_launch(b, stream);
+                cudaEventRecord(e1, s);
+                if (cudaEventSynchronize(e1) != cudaSuccess) {
+                    bine_batch_destroy(b);
+                    rc = fail(BINE_ERR_CUDA, "autotune launch failed");
+                    goto done;
+                }
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= reps;
+                if (ms < best_t) {
+                    best_t = ms;
+                    *best = tu;
+                }
+                bine_batch_destroy(b);
+            }
+        }
+    }
+done:
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best_ms) *best_ms = best_t;
+    return rc;
+}
 
 const char* bine_last_error_string(void) { return g_err.c_str(); }
 

@@ -512,9 +512,9 @@ __global__ void __launch_bounds__(kThreads) k_steps(StepBufs B, const StepMove* 
 
 // ------------------------------------------------------ torus link bytes
 // Per-link byte accounting of a schedule on the communicator's torus.  A
-// message moves along one dimension only (Bine and recursive-doubling peers
-// differ in one coordinate) and takes the minimal ring route, the +
-// direction on ties.  Link (node, d, dir) has index (node*ndims + d)*2 + dir
+// message takes the dimension-ordered route, minimal on each ring, the +
+// direction on ties (Bine and recursive-doubling peers differ in one
+// coordinate; 1-D algorithms on a torus may differ in several).  Link (node, d, dir) has index (node*ndims + d)*2 + dir
 // (dir 0: +, 1: -).  Each message adds its bytes to a cyclic range of link
 // positions on one ring, recorded as two or three signed updates of a
 // difference array (unsigned wrap-around arithmetic, exact mod 2^64); one
@@ -529,38 +529,40 @@ __device__ __forceinline__ size_t link_index(const Torus& t, int node, int d, in
     return ((size_t)node * t.ndims + d) * 2 + dir;
 }
 
-// Adds `bytes` to the links of the minimal route src -> dst.
+// Adds `bytes` to the links of the route src -> dst: dimension-ordered
+// (dimension 0 first), minimal in each dimension, + direction on ties.
 __device__ __forceinline__ void add_route(const Torus& t, int src, int dst, unsigned long long bytes,
                                           unsigned long long* diff) {
     if (src == dst || bytes == 0) return;
     int a[kMaxDims] = {0, 0, 0}, b[kMaxDims] = {0, 0, 0};
     t.coords(src, a);
     t.coords(dst, b);
-    int d = -1;
-    for (int i = 0; i < t.ndims; i++)
-        if (a[i] != b[i]) d = i;
-    if (d < 0) return;
-    const int L = t.dims[d];
-    const int delta = pmod(b[d] - a[d], L);
-    int dir = 0, start = a[d], hops = delta;
-    if (L - delta < delta) {  // minus direction: positions a-h+1 .. a
-        dir = 1;
-        hops = L - delta;
-        start = pmod(a[d] - hops + 1, L);
-    }
     int c[kMaxDims] = {a[0], a[1], a[2]};
-    auto at = [&](int pos) {
-        c[d] = pos;
-        return link_index(t, t.id(c), d, dir);
-    };
     const unsigned long long neg = 0ull - bytes;
-    const int end = start + hops;  // exclusive
-    atomicAdd(&diff[at(start)], bytes);
-    if (end < L) {
-        atomicAdd(&diff[at(end)], neg);
-    } else if (end > L) {  // wraps: [start, L) and [0, end - L)
-        atomicAdd(&diff[at(0)], bytes);
-        atomicAdd(&diff[at(end - L)], neg);
+    for (int d = 0; d < t.ndims; d++) {
+        if (c[d] == b[d]) continue;
+        const int L = t.dims[d];
+        const int delta = pmod(b[d] - c[d], L);
+        int dir = 0, start = c[d], hops = delta;
+        if (L - delta < delta) {  // minus direction: positions c-h+1 .. c
+            dir = 1;
+            hops = L - delta;
+            start = pmod(c[d] - hops + 1, L);
+        }
+        auto at = [&](int pos) {
+            int q[kMaxDims] = {c[0], c[1], c[2]};
+            q[d] = pos;
+            return link_index(t, t.id(q), d, dir);
+        };
+        const int end = start + hops;  // exclusive
+        atomicAdd(&diff[at(start)], bytes);
+        if (end < L) {
+            atomicAdd(&diff[at(end)], neg);
+        } else if (end > L) {  // wraps: [start, L) and [0, end - L)
+            atomicAdd(&diff[at(0)], bytes);
+            atomicAdd(&diff[at(end - L)], neg);
+        }
+        c[d] = b[d];
     }
 }
 
@@ -660,6 +662,109 @@ __global__ void k_link_scan(Torus t, unsigned long long* links) {
             acc += links[li];
             links[li] = acc;
         }
+    }
+}
+
+}  // namespace dev
+}  // namespace bine
+
+// --------------------------------------------------------- batched launch
+// Thousands of independent allreduce / reduce_scatter / allgather calls of
+// different P, sizes and element types in ONE persistent launch.  Every
+// call is cut into tiles; blocks take tiles grid-stride from the global tile
+// range and find their call by binary search over tile_begin.  Reduction
+// tiles are `tc` 16-byte columns wide and split the P rows over 256/tc warps
+// groups (tc comes from the autotuner: narrow tiles with many row groups for
+// large P, wide tiles for small P); allgather tiles are 256 vectors of the
+// flattened (source rank, column) space, each stored to all P rows.
+// Integer sums wrap, float32 sums accumulate in FP64 (the FAST order).
+namespace bine {
+namespace dev {
+
+enum BatchOp { kBatchAllreduce = 0, kBatchReduceScatter = 1, kBatchAllgather = 2 };
+
+struct BatchItem {
+    const char* in;
+    char* out;
+    long long in_stride, out_stride;  // bytes between rank rows
+    long long ncol;                   // 16-byte vectors per input row
+    long long blk;                    // reduce_scatter: vectors per destination rank
+    long long tile_begin, ntiles;
+    int P, op, is_float, tc;
+};
+
+template <typename T, typename A>
+__device__ __forceinline__ void batch_reduce_tile(const BatchItem& it, long long tile, Lanes<float, double>* part_f,
+                                                  uint4* res) {
+    const int tc = it.tc, groups = kThreads / tc;
+    const int lane = threadIdx.x % tc, grp = threadIdx.x / tc;
+    const int per = (it.P + groups - 1) / groups;
+    const int r0 = min(it.P, grp * per), r1 = min(it.P, r0 + per);
+    const long long col = tile * tc + lane;
+    Lanes<T, A> acc;
+    acc.zero();
+    if (col < it.ncol) {
+        const char* p = it.in + col * 16;
+        int r = r0;
+        for (; r + 8 <= r1; r += 8) {
+            uint4 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = ld_stream(p + (long long)(r + u) * it.in_stride);
+#pragma unroll
+            for (int u = 0; u < 8; u++) acc.add(v[u]);
+        }
+        for (; r < r1; r++) acc.add(ld_stream(p + (long long)r * it.in_stride));
+    }
+    Lanes<T, A>* part = reinterpret_cast<Lanes<T, A>*>(part_f);
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    if (grp == 0) {
+        Lanes<T, A> s = part[lane];
+        for (int g = 1; g < groups; g++)
+#pragma unroll
+            for (int i = 0; i < Lanes<T, A>::N; i++) s.v[i] = add_exact<A>(s.v[i], part[g * tc + lane].v[i]);
+        res[lane] = s.pack();
+    }
+    __syncthreads();
+    if (col < it.ncol) {
+        const uint4 v = res[lane];
+        if (it.op == kBatchAllreduce) {
+            char* q = it.out + col * 16;
+            for (int d = grp; d < it.P; d += groups) st_stream(q + (long long)d * it.out_stride, v);
+        } else if (grp == 0) {
+            const long long owner = col / it.blk;
+            st_stream(it.out + owner * it.out_stride + (col - owner * it.blk) * 16, v);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_batch(const BatchItem* __restrict__ items, int nitems,
+                                                    long long total_tiles) {
+    __shared__ Lanes<float, double> part[kThreads];
+    __shared__ uint4 res[kThreads];
+    for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        int lo = 0, hi = nitems - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (items[mid].tile_begin <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchItem it = items[lo];
+        const long long tile = t - it.tile_begin;
+        if (it.op == kBatchAllgather) {
+            const long long idx = tile * kThreads + threadIdx.x;
+            if (idx < (long long)it.P * it.ncol) {
+                const long long i = idx / it.ncol, j = idx - (idx / it.ncol) * it.ncol;
+                const uint4 v = ld_stream(it.in + i * it.in_stride + j * 16);
+                char* q = it.out + (i * it.ncol + j) * 16;
+                for (int d = 0; d < it.P; d++) st_stream(q + (long long)d * it.out_stride, v);
+            }
+        } else if (it.is_float) {
+            batch_reduce_tile<float, double>(it, tile, part, res);
+        } else {
+            batch_reduce_tile<int32_t, int32_t>(it, tile, part, res);
+        }
+        __syncthreads();
     }
 }
 

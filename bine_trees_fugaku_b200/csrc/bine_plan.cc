@@ -1619,33 +1619,32 @@ bool Planner::verify(const PlanKey& k, const Schedule& s, std::string* err) cons
 
 bool link_bytes(const Torus& t, const std::vector<Message>& msgs, int es, std::vector<uint64_t>* out,
                 std::string* err) {
+    (void)err;
     out->assign((size_t)t.size * t.ndims * 2, 0);
     for (const Message& m : msgs) {
         if (m.src == m.dst || m.elems == 0) continue;
-        int a[kMaxDims], b[kMaxDims];
+        int a[kMaxDims] = {0, 0, 0}, b[kMaxDims] = {0, 0, 0};
         t.coords(m.src, a);
         t.coords(m.dst, b);
-        int dim = -1;
-        for (int d = 0; d < t.ndims; d++)
-            if (a[d] != b[d]) {
-                if (dim >= 0) {
-                    *err = "a message changes more than one coordinate";
-                    return false;
-                }
-                dim = d;
-            }
-        const int L = t.dims[dim];
-        int delta = pmod(b[dim] - a[dim], L);  // hops in + direction
-        int dir = 1, hops = delta;
-        if (L - delta < delta) {
-            dir = -1;
-            hops = L - delta;
-        }
+        // Dimension-ordered route (dimension 0 first), minimal in each
+        // dimension, the + direction on ties.  Bine and recursive-doubling
+        // peers differ in one coordinate; 1-D algorithms run on a torus
+        // (alltoall, scatter, gather) may differ in several.
         int c[kMaxDims] = {a[0], a[1], a[2]};
-        for (int h = 0; h < hops; h++) {
-            size_t link = ((size_t)t.id(c) * t.ndims + dim) * 2 + (dir > 0 ? 0 : 1);
-            (*out)[link] += (uint64_t)m.elems * es;
-            c[dim] = pmod(c[dim] + dir, L);
+        for (int dim = 0; dim < t.ndims; dim++) {
+            if (c[dim] == b[dim]) continue;
+            const int L = t.dims[dim];
+            int delta = pmod(b[dim] - c[dim], L);
+            int dir = 1, hops = delta;
+            if (L - delta < delta) {
+                dir = -1;
+                hops = L - delta;
+            }
+            for (int h = 0; h < hops; h++) {
+                size_t link = ((size_t)t.id(c) * t.ndims + dim) * 2 + (dir > 0 ? 0 : 1);
+                (*out)[link] += (uint64_t)m.elems * es;
+                c[dim] = pmod(c[dim] + dir, L);
+            }
         }
     }
     return true;

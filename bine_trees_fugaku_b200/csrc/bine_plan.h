@@ -149,7 +149,7 @@ class Planner {
 
 // Per-link byte counts of a message list on the torus: 2 * ndims directed
 // links per node, index (node * ndims + d) * 2 + (dir > 0 ? 0 : 1).
-// Returns false if some message moves along more than one dimension.
+// Routes are dimension-ordered and minimal per dimension (+ on ties).
 bool link_bytes(const Torus& t, const std::vector<Message>& msgs, int elem_size, std::vector<uint64_t>* out,
                 std::string* err);
 

