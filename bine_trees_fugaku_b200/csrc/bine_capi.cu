@@ -550,6 +550,118 @@ int plan_for_query(bine_comm_t c, int coll, long count, int root, std::shared_pt
 
 }  // namespace
 
+// ------------------------------------------------------- allocation-free call
+// Callers that cannot allocate device memory (code running under a memory
+// manager that owns every allocation, allocators that forbid cudaMalloc
+// during steady state, or code that must not touch the CUDA heap at all)
+// can still run the step engine through bine_allreduce_noalloc(): its
+// schedule tables, grid-barrier words and workspace rows live in this one
+// fixed array, which the CUDA runtime reserves when the library's module is
+// loaded on a device and keeps until the process exits.
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // 64 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current (host code may not use the symbol itself: on the
+// host it is only a stand-in for the device array).
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+int noalloc_scratch(int dev, char** out) {
+    if (dev < 0 || dev >= kMaxDevices) return fail(BINE_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(BINE_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = (char*)g_noalloc_ptr[dev];
+    return BINE_SUCCESS;
+}
+
+size_t round256(size_t x) { return (x + 255) / 256 * 256; }
+
+template <typename T>
+int noalloc_run(bine_comm_t c, const Schedule& s, const char* send, long long ist, char* recv, long long ost,
+                int dev) {
+    // Scratch layout: [barrier u32 x2 | status i32] [level_begin] [moves] [chunks] [workspace rows].
+    std::vector<dev::StepMove> moves;
+    std::vector<dev::StepChunk> chunks;
+    std::vector<int> lb;
+    int max_chunks = 0;
+    const int64_t chunk_elems = std::max<int64_t>(16, (32 * 1024) / (int64_t)sizeof(T));
+    for (const auto& lvl : s.levels) {
+        lb.push_back((int)chunks.size());
+        for (const Move& m : lvl) {
+            dev::StepMove dm{m.dst.off, m.a.off, m.b.off, m.dst.rank, m.a.rank, m.b.rank, m.dst.buf, m.a.buf, m.b.buf,
+                             m.add};
+            const int mi = (int)moves.size();
+            moves.push_back(dm);
+            for (int64_t st = 0; st < m.n; st += chunk_elems)
+                chunks.push_back(dev::StepChunk{mi, 0, st, std::min(chunk_elems, m.n - st)});
+        }
+        max_chunks = std::max(max_chunks, (int)chunks.size() - lb.back());
+    }
+    lb.push_back((int)chunks.size());
+    const size_t tmp_stride = round256((size_t)s.tmp_elems * sizeof(T));
+    const size_t off_lb = 256, off_mv = off_lb + round256(lb.size() * sizeof(int));
+    const size_t off_ch = off_mv + round256(moves.size() * sizeof(dev::StepMove));
+    const size_t off_ws = off_ch + round256(chunks.size() * sizeof(dev::StepChunk));
+    const size_t need = off_ws + tmp_stride * (size_t)c->P;
+    if (need > kNoAllocScratchBytes)
+        return fail(BINE_ERR_NOMEM, "bine_allreduce_noalloc: this call needs " + std::to_string(need) +
+                                        " bytes of scratch, more than the fixed " +
+                                        std::to_string(kNoAllocScratchBytes) + " bytes; use bine_allreduce");
+    char* base = nullptr;
+    int rc = noalloc_scratch(dev, &base);
+    if (rc) return rc;
+    cudaStream_t st = c->stream;
+    // The barrier words and the status word must start at zero on every call.
+    CUDA_TRY(cudaMemsetAsync(base, 0, 256, st));
+    CUDA_TRY(cudaMemcpyAsync(base + off_lb, lb.data(), lb.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (!moves.empty())
+        CUDA_TRY(cudaMemcpyAsync(base + off_mv, moves.data(), moves.size() * sizeof(dev::StepMove),
+                                 cudaMemcpyHostToDevice, st));
+    if (!chunks.empty())
+        CUDA_TRY(cudaMemcpyAsync(base + off_ch, chunks.data(), chunks.size() * sizeof(dev::StepChunk),
+                                 cudaMemcpyHostToDevice, st));
+    dev::StepBufs B;
+    B.base[kBufSend] = const_cast<char*>(send);
+    B.base[kBufRecv] = recv;
+    B.base[kBufTmp] = base + off_ws;
+    B.stride[kBufSend] = ist;
+    B.stride[kBufRecv] = ost;
+    B.stride[kBufTmp] = (long long)tmp_stride;
+    int sms = 0, per_sm = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_steps<T>, dev::kThreads, 0));
+    int blocks = std::max(1, std::min(per_sm * sms, std::max(1, max_chunks)));
+    const dev::StepMove* mv = (const dev::StepMove*)(base + off_mv);
+    const dev::StepChunk* ch = (const dev::StepChunk*)(base + off_ch);
+    const int* lbp = (const int*)(base + off_lb);
+    int nl = (int)s.levels.size();
+    unsigned* bar = (unsigned*)base;
+    int* status = (int*)(base + 16);
+    unsigned long long to = c->step_timeout_ns;
+    unsigned expected = (unsigned)blocks;
+    void* args[] = {&B, &mv, &ch, &lbp, &nl, &bar, &status, &to, &expected};
+    CUDA_TRY(cudaLaunchCooperativeKernel((void*)dev::k_steps<T>, dim3(blocks), dim3(dev::kThreads), args, 0, st));
+    // The host staging of the tables and the status check need the call to
+    // finish before returning.
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int stv = 0;
+    CUDA_TRY(cudaMemcpy(&stv, status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (stv != dev::kStepOk) return fail(BINE_ERR_TIMEOUT, "a grid barrier of the step engine timed out");
+    return BINE_SUCCESS;
+}
+
+}  // namespace
+
 // ---------------------------------------------------------------- batches
 struct bine_batch_s {
     dev::BatchItem* items = nullptr;
@@ -736,6 +848,46 @@ done:
 }
 
 const char* bine_last_error_string(void) { return g_err.c_str(); }
+
+int bine_allreduce_noalloc(const void* sendbuf, void* recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
+                           bine_comm_t comm) {
+    if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    const int es = dtype_size(datatype);
+    if (es < 0) return fail(BINE_ERR_ARG, "invalid datatype");
+    if (count < 0) return fail(BINE_ERR_ARG, "negative count");
+    if (count == 0) return BINE_SUCCESS;
+    if (!sendbuf || !recvbuf) return fail(BINE_ERR_ARG, "null buffer");
+    const long long ist = comm->send_stride ? (long long)comm->send_stride : (long long)count * es;
+    const long long ost = comm->recv_stride ? (long long)comm->recv_stride : (long long)count * es;
+    if (ist < (long long)count * es || ost < (long long)count * es)
+        return fail(BINE_ERR_ARG, "layout stride smaller than a rank row");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    const PlanKey k = make_key(comm, kAllreduce, count, 0);
+    std::shared_ptr<Schedule> s;
+    int rc = get_schedule(comm, k, &s);
+    if (rc) return rc;
+    std::string verr;
+    if (!comm->planner->verify(k, *s, &verr)) return fail(BINE_ERR_UNSUPPORTED, verr);
+    const int64_t rows[3] = {s->send_elems, s->recv_elems, s->tmp_elems};
+    for (const auto& lvl : s->levels)
+        for (const Move& m : lvl)
+            for (const Region* r : {&m.dst, &m.a, &m.b})
+                if (r->rank < 0 || r->rank >= comm->P || r->buf > kBufTmp || r->off < 0 || m.n < 0 ||
+                    r->off + m.n > rows[r->buf])
+                    return fail(BINE_ERR_INTERNAL, "planner produced a region outside its buffer row");
+    const char* in = (const char*)sendbuf;
+    char* out = (char*)recvbuf;
+    switch (datatype) {
+    case BINE_INT32: return noalloc_run<int32_t>(comm, *s, in, ist, out, ost, dev);
+    case BINE_INT64: return noalloc_run<int64_t>(comm, *s, in, ist, out, ost, dev);
+    case BINE_FLOAT: return noalloc_run<float>(comm, *s, in, ist, out, ost, dev);
+    case BINE_DOUBLE: return noalloc_run<double>(comm, *s, in, ist, out, ost, dev);
+    case BINE_CHAR: return noalloc_run<int8_t>(comm, *s, in, ist, out, ost, dev);
+    }
+    return fail(BINE_ERR_ARG, "invalid datatype");
+}
 
 int bine_comm_create(int nranks, int ndims, const int* dims, bine_comm_t* comm) {
     if (!comm) return fail(BINE_ERR_ARG, "null output pointer");

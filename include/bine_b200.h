@@ -153,6 +153,30 @@ int bine_gather(const void *sendbuf, int sendcount, bine_datatype_t sendtype, vo
 int bine_reduce(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op, int root,
                 bine_comm_t comm);
 
+/* Allocation-free allreduce.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory -- code running inside a
+ * memory manager that owns every device allocation, or in a phase where
+ * cudaMalloc is forbidden -- and so cannot let bine_allreduce() create its
+ * workspace and schedule tables on first use.  It runs the same STEPS
+ * engine schedule as bine_allreduce() with BINE_ENGINE_STEPS (the
+ * communicator's allreduce variant, ports and layout), but every piece of
+ * device scratch it needs -- the schedule tables, the grid-barrier and
+ * status words and the workspace rows -- lives in one fixed 64 MiB array
+ * that the library reserves on each device that loads it and keeps until
+ * the process exits.  It calls no cudaMalloc, cudaFree or other allocating
+ * routine.  The caller passes the input and output arrays as usual.
+ *   * Calls needing more than 64 MiB of scratch (schedule tables plus
+ *     workspace; the B variant's tables grow with nranks squared) fail with
+ *     BINE_ERR_NOMEM and a message naming the size.
+ *   * The first call on a device looks up the array's device address; make
+ *     that first call before any stream capture.
+ *   * Every call reuses the same array: two calls that overlap on the GPU
+ *     (on different streams or from different threads) race.  The call is
+ *     synchronous: it returns after its kernel finished and reports a
+ *     barrier timeout as BINE_ERR_TIMEOUT. */
+int bine_allreduce_noalloc(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
+                           bine_comm_t comm);
+
 /* Waits for the communicator's stream and reports device-side errors
  * (BINE_ERR_TIMEOUT when a bounded barrier of the STEPS engine expired). */
 int bine_comm_synchronize(bine_comm_t comm);
