@@ -97,6 +97,7 @@ def lib():
     L = ctypes.CDLL(LIB_PATH)
     vp, i, ci, sz, i64p = ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64)
     L.bine_last_error_string.restype = ctypes.c_char_p
+    L.bine_mlp_last_error.restype = ctypes.c_char_p
     sig = {
         "bine_comm_create": [i, i, ctypes.POINTER(ci), ctypes.POINTER(vp)],
         "bine_comm_destroy": [vp],
@@ -105,6 +106,7 @@ def lib():
         "bine_comm_set_ports": [vp, i],
         "bine_comm_set_algo": [vp, i, i, i, i],
         "bine_comm_set_engine": [vp, i],
+        "bine_comm_set_segment": [vp, ctypes.c_longlong],
         "bine_comm_set_float_order": [vp, i],
         "bine_comm_set_step_timeout": [vp, ctypes.c_uint],
         "bine_debug_set_barrier_extra": [vp, ctypes.c_uint],
@@ -124,6 +126,14 @@ def lib():
         "bine_plan_messages": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz)],
         "bine_plan_trees": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz)],
         "bine_link_bytes_host": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(ctypes.c_uint64), sz],
+        "bine_mlp_create": [i, i, i, i, ctypes.c_ulonglong, ctypes.POINTER(vp)],
+        "bine_mlp_destroy": [vp],
+        "bine_mlp_num_params": [vp, ctypes.POINTER(sz)],
+        "bine_mlp_get_params": [vp, vp],
+        "bine_mlp_set_params": [vp, vp],
+        "bine_mlp_forward": [vp, vp, i, vp, vp],
+        "bine_mlp_gradients": [vp, vp, vp, vp, i, vp, ctypes.POINTER(ctypes.c_float)],
+        "bine_mlp_train_step": [vp, vp, vp, vp, i, ctypes.c_float, vp, ctypes.POINTER(ctypes.c_float)],
         "bine_batch_create": [ctypes.POINTER(BatchItem), i, ctypes.POINTER(BatchTuning), ctypes.POINTER(vp)],
         "bine_batch_launch": [vp, vp],
         "bine_batch_destroy": [vp],
@@ -213,6 +223,9 @@ class Comm:
 
     def set_engine(self, engine):
         check(lib().bine_comm_set_engine(self._h, {"fused": ENGINE_FUSED, "steps": ENGINE_STEPS}.get(engine, engine)))
+
+    def set_segment(self, segment_bytes):
+        check(lib().bine_comm_set_segment(self._h, segment_bytes))
 
     def set_float_order(self, order):
         check(lib().bine_comm_set_float_order(self._h, {"reference": ORDER_REFERENCE, "fast": ORDER_FAST}.get(order, order)))
@@ -391,3 +404,77 @@ class Batch:
         h = stream if isinstance(stream, int) else (stream.cuda_stream if stream is not None else 0)
         check(lib().bine_batch_autotune(arr, len(items), h, reps, ctypes.byref(best), ctypes.byref(ms)))
         return best, ms.value
+
+
+class MLP:
+    """bine_mlp_*: in -> H -> H -> H -> out MLP (GELU, bf16 weights and
+    activations, fp32 accumulation) trained with the engine's own kernels."""
+
+    def __init__(self, in_dim, hidden, out_dim, max_batch, seed=0):
+        self.dims = (in_dim, hidden, out_dim)
+        self.max_batch = max_batch
+        self._h = ctypes.c_void_p()
+        self._check(lib().bine_mlp_create(in_dim, hidden, out_dim, max_batch, seed, ctypes.byref(self._h)))
+        n = ctypes.c_size_t()
+        self._check(lib().bine_mlp_num_params(self._h, ctypes.byref(n)))
+        self.nparams = n.value
+
+    def _check(self, rc):
+        if rc != SUCCESS:
+            raise BineError(rc, lib().bine_mlp_last_error().decode())
+
+    def layout(self):
+        """(weight offset, bias offset, out, in) per layer in the parameter arena."""
+        din, h, dout = self.dims
+        dims = [din, h, h, h, dout]
+        off, out = 0, []
+        for l in range(4):
+            w = off
+            off = (off + dims[l] * dims[l + 1] + 15) // 16 * 16
+            b = off
+            off = (off + dims[l + 1] + 15) // 16 * 16
+            out.append((w, b, dims[l + 1], dims[l]))
+        return out
+
+    def get_params(self):
+        out = np.zeros(self.nparams, np.float32)
+        self._check(lib().bine_mlp_get_params(self._h, out.ctypes.data))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparams
+        self._check(lib().bine_mlp_set_params(self._h, p.ctypes.data))
+
+    def forward(self, x, stream=None):
+        """x: CUDA float32 tensor [n, in] (n multiple of 16) -> [n, out]."""
+        import torch
+        y = torch.empty((x.shape[0], self.dims[2]), dtype=torch.float32, device=x.device)
+        h = stream.cuda_stream if stream is not None else 0
+        self._check(lib().bine_mlp_forward(self._h, x.data_ptr(), x.shape[0], y.data_ptr(), h))
+        return y
+
+    def gradients(self, x, t, mask):
+        g = np.zeros(self.nparams, np.float32)
+        loss = ctypes.c_float()
+        self._check(lib().bine_mlp_gradients(self._h, x.data_ptr(), t.data_ptr(), mask.data_ptr(), x.shape[0],
+                                             g.ctypes.data, ctypes.byref(loss)))
+        return g, loss.value
+
+    def train_step(self, x, t, mask, lr, stream=None):
+        loss = ctypes.c_float()
+        h = stream.cuda_stream if stream is not None else 0
+        self._check(lib().bine_mlp_train_step(self._h, x.data_ptr(), t.data_ptr(), mask.data_ptr(), x.shape[0], lr,
+                                              h, ctypes.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bine_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -91,10 +91,31 @@ struct DevTrees {
 struct PlanKeyEs {
     PlanKey k;
     int es;
-    bool operator==(const PlanKeyEs& o) const { return k == o.k && es == o.es; }
+    long long segment;  // step engine: bytes per work chunk (0: 32 KiB)
+    bool operator==(const PlanKeyEs& o) const { return k == o.k && es == o.es && segment == o.segment; }
 };
 struct PlanKeyEsHash {
-    size_t operator()(const PlanKeyEs& x) const { return PlanKeyHash()(x.k) * 31 + (size_t)x.es; }
+    size_t operator()(const PlanKeyEs& x) const {
+        return PlanKeyHash()(x.k) * 31 + (size_t)x.es + (size_t)x.segment * 7919;
+    }
+};
+
+// A schedule's routing does not depend on `count` once every block is
+// non-empty, so one symbolic proof covers every count of the same
+// structure (collective, variant, family, distance, ports, root) and
+// block-occupancy class.
+struct StructKey {
+    int coll, variant, family, distance, ports, root, full;
+    bool operator==(const StructKey& o) const {
+        return coll == o.coll && variant == o.variant && family == o.family && distance == o.distance &&
+               ports == o.ports && root == o.root && full == o.full;
+    }
+};
+struct StructKeyHash {
+    size_t operator()(const StructKey& k) const {
+        return (size_t)k.coll * 1000003u ^ (size_t)k.variant * 10007u ^ (size_t)k.family * 101u ^
+               (size_t)k.distance * 13u ^ (size_t)k.ports * 7u ^ (size_t)(k.root + 1) * 999983u ^ (size_t)k.full;
+    }
 };
 
 }  // namespace
@@ -112,6 +133,9 @@ struct bine_comm_s {
     std::unordered_map<PlanKey, std::shared_ptr<Schedule>, PlanKeyHash> schedules;
     std::unordered_map<PlanKeyEs, std::shared_ptr<DevSteps>, PlanKeyEsHash> dev_steps;
     std::unordered_map<PlanKeyEs, std::shared_ptr<DevTrees>, PlanKeyEsHash> dev_trees;
+    std::unordered_map<StructKey, int, StructKeyHash> verified;  // 1: proven, 0: refuted
+    std::unordered_map<StructKey, std::string, StructKeyHash> refuted_why;
+    long long segment_bytes = 0;
     // Device state, created on first use.
     int device = -1;
     int num_sms = 0;
@@ -188,21 +212,41 @@ void fill(T** dptr, const std::vector<T>& v, cudaError_t* err) {
     if (*err == cudaSuccess && !v.empty()) *err = cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
 
+// Proves (once per structure, see StructKey) that schedule `s` computes the
+// MPI result.
+int verify_cached(bine_comm_t c, const PlanKey& k, const Schedule& s) {
+    StructKey sk{k.coll, k.variant, k.family, k.distance, k.ports, k.root, k.count >= (int64_t)k.ports * c->P ? 1 : 0};
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        auto it = c->verified.find(sk);
+        if (it != c->verified.end()) {
+            if (it->second) return BINE_SUCCESS;
+            return fail(BINE_ERR_UNSUPPORTED, c->refuted_why[sk]);
+        }
+    }
+    std::string verr;
+    const bool ok = c->planner->verify(k, s, &verr);
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->verified[sk] = ok ? 1 : 0;
+    if (!ok) {
+        c->refuted_why[sk] = verr;
+        return fail(BINE_ERR_UNSUPPORTED, verr);
+    }
+    return BINE_SUCCESS;
+}
+
 int get_dev_steps(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSteps>* out) {
     std::shared_ptr<Schedule> s;
     int rc = get_schedule(c, k, &s);
     if (rc) return rc;
+    rc = verify_cached(c, k, *s);
+    if (rc) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
-    PlanKeyEs key{k, es};
+    PlanKeyEs key{k, es, c->segment_bytes};
     auto it = c->dev_steps.find(key);
     if (it != c->dev_steps.end()) {
         *out = it->second;
         return BINE_SUCCESS;
-    }
-    // The STEPS engine only runs schedules proven to compute the MPI result.
-    {
-        std::string verr;
-        if (!c->planner->verify(k, *s, &verr)) return fail(BINE_ERR_UNSUPPORTED, verr);
     }
     // Every region the kernel will touch must lie inside its row: a planner
     // error must never become an out-of-bounds device access.
@@ -217,7 +261,8 @@ int get_dev_steps(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSt
     std::vector<dev::StepMove> moves;
     std::vector<dev::StepChunk> chunks;
     std::vector<int> lb;
-    const int64_t chunk_elems = std::max<int64_t>(16, (32 * 1024) / es);
+    const int64_t seg = c->segment_bytes > 0 ? c->segment_bytes : 32 * 1024;
+    const int64_t chunk_elems = std::max<int64_t>(16, seg / es);
     for (const auto& lvl : s->levels) {
         lb.push_back((int)chunks.size());
         for (const Move& m : lvl) {
@@ -259,7 +304,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
     int rc = get_schedule(c, k, &s);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
-    PlanKeyEs key{k, es};
+    PlanKeyEs key{k, es, 0};
     auto it = c->dev_trees.find(key);
     if (it != c->dev_trees.end()) {
         *out = it->second;
@@ -964,6 +1009,13 @@ int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int fami
     if (coll == BINE_COLL_BCAST && variant == kBcScatterAllgather && distance == BINE_DISTANCE_DEFAULT)
         cf.distance = kIncreasing;
     comm->cfg[coll] = cf;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (segment_bytes < 0) return fail(BINE_ERR_ARG, "segment size must be >= 0");
+    comm->segment_bytes = segment_bytes;
     return BINE_SUCCESS;
 }
 

@@ -115,6 +115,12 @@ int bine_comm_set_ports(bine_comm_t comm, int ports);
 int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int family, int distance);
 
 int bine_comm_set_engine(bine_comm_t comm, int engine);
+
+/* LIBBINE_SEGMENT_SIZE analogue for the STEPS engine: bytes of each unit of
+ * work a block takes (0: 32 KiB).  Small segments spread small messages
+ * over more blocks; large ones cut per-chunk overhead.  Results do not
+ * depend on it. */
+int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes);
 int bine_comm_set_float_order(bine_comm_t comm, int order);
 
 /* ----------------------------------------------------------- collectives */
@@ -243,6 +249,32 @@ int bine_batch_destroy(bine_batch_t batch);
  * CUDA events) and returns the fastest in *best and its time in *best_ms. */
 int bine_batch_autotune(const bine_batch_item_t *items, int nitems, void *stream, int reps,
                         bine_batch_tuning_t *best, float *best_ms);
+
+/* -------------------------------------------------------- learned picker
+ * A 3-hidden-layer MLP (in -> H -> H -> H -> out, GELU, bf16 weights and
+ * activations, fp32 accumulation) with forward, backward and Adam kernels.
+ * The engine's variant picker (bine_trees_fugaku_b200/picker.py) trains it
+ * on timings and link-byte counts the engine itself measures and uses it to
+ * choose variant, port count and segment size per call.  Not in the
+ * reference.  All dimensions and batch sizes are multiples of 16; device
+ * pointers are fp32 row-major [n x in] / [n x out]. */
+typedef struct bine_mlp_s *bine_mlp_t;
+int bine_mlp_create(int in_dim, int hidden, int out_dim, int max_batch, unsigned long long seed, bine_mlp_t *mlp);
+int bine_mlp_destroy(bine_mlp_t mlp);
+int bine_mlp_num_params(bine_mlp_t mlp, size_t *n);
+/* Parameter arena: for layer l, weights [out x in] row-major then the bias,
+ * each starting at a multiple of 16 floats (fp32 masters). */
+int bine_mlp_get_params(bine_mlp_t mlp, float *host);
+int bine_mlp_set_params(bine_mlp_t mlp, const float *host);
+int bine_mlp_forward(bine_mlp_t mlp, const float *d_x, int n, float *d_y, void *stream);
+/* Gradients of the masked mean squared error (same layout as the
+ * parameters), for checking against a CPU reference. */
+int bine_mlp_gradients(bine_mlp_t mlp, const float *d_x, const float *d_t, const float *d_mask, int n,
+                       float *host_grads, float *loss);
+/* One Adam step on a batch; *loss receives the batch loss (synchronous). */
+int bine_mlp_train_step(bine_mlp_t mlp, const float *d_x, const float *d_t, const float *d_mask, int n, float lr,
+                        void *stream, float *loss);
+const char *bine_mlp_last_error(void);
 
 /* ------------------------------------------------------ schedule queries
  * Host-only: these plan the call with the communicator's current settings
