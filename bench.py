@@ -413,6 +413,35 @@ def run_batch_suite(args):
     e1.record(stream)
     torch.cuda.synchronize()
     per_call_ms = e0.elapsed_time(e1) / reps
+    # The same per-call launches captured in one CUDA graph: no host
+    # launch overhead, still one kernel per collective.
+    per_call_graph_ms = None
+    try:
+        g1 = torch.cuda.CUDAGraph()
+        s1 = torch.cuda.Stream()
+        s1.wait_stream(stream)
+        for cm in comms.values():
+            cm.set_stream(s1)
+        with torch.cuda.stream(s1):
+            with torch.cuda.graph(g1, stream=s1):
+                per_call()
+        stream.wait_stream(s1)
+        for cm in comms.values():
+            cm.set_stream(stream)
+        for _ in range(3):
+            g1.replay()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            g1.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        per_call_graph_ms = e0.elapsed_time(e1) / reps
+        del g1
+    except (RuntimeError, bine.BineError) as e:
+        print(f"per-call graph capture failed: {e}", file=sys.stderr)
+        for cm in comms.values():
+            cm.set_stream(stream)
 
     # Autotuned batched launch (tuning cached on disk with a checksum).
     cache = os.path.join(ROOT, "gpurun_out", "batch_tuning.json") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) \
@@ -455,7 +484,9 @@ def run_batch_suite(args):
             "value": algo_bytes / (batch_ms * 1e-3) / 1e9,
             "per_call_value": algo_bytes / (per_call_ms * 1e-3) / 1e9,
             "speedup_vs_one_launch_per_collective": per_call_ms / batch_ms,
-            "batch_ms": batch_ms, "per_call_ms": per_call_ms, "collectives": len(items),
+            "speedup_vs_one_launch_per_collective_graph": (per_call_graph_ms / batch_ms) if per_call_graph_ms else None,
+            "batch_ms": batch_ms, "per_call_ms": per_call_ms, "per_call_graph_ms": per_call_graph_ms,
+            "collectives": len(items),
             "collectives_per_s": len(items) / (batch_ms * 1e-3),
             "integer_results_equal_single_calls": exact,
             "config": {"n": len(items), "P": "U[4,512]", "message": f"log-uniform [64 B, {upper} B] (per-rank, larger buffer)",
@@ -465,6 +496,73 @@ def run_batch_suite(args):
     print(json.dumps(line))
     batch.close()
     return 0 if exact else 1
+
+
+def run_picker_suite(args):
+    """Learned variant picker: measures every valid arm of sampled calls on
+    the GPU (STEPS engine times, device link accounting), trains bine_mlp on
+    80% of the calls and judges its picks on the held-out 20% against
+    exhaustive search and the fixed rule.  --picker-data reuses a measured
+    dataset instead of measuring."""
+    import numpy as np
+    import torch
+
+    import bine_trees_fugaku_b200 as bine
+    from bine_trees_fugaku_b200 import picker as pk
+
+    torch.cuda.set_device(0)
+    out_dir = args.out or os.path.join(ROOT, "gpurun_out")
+    os.makedirs(out_dir, exist_ok=True)
+
+    def log(m):
+        print(m, file=sys.stderr, flush=True)
+
+    t0 = time.time()
+    if args.picker_data:
+        z = np.load(args.picker_data)
+        cfgs = json.loads(str(z["configs"]))
+        X, T, Lb, valid = z["X"], z["T"].astype(np.float64), z["Lb"], z["valid"]
+        te = z["test"]
+    else:
+        configs = pk.sample_configs(args.picker_n, seed=args.picker_seed)
+        cfgs, X, T, Lb, valid = pk.measure(configs, reps=3, time_budget_s=args.picker_budget, log=log)
+        perm = np.random.default_rng(5).permutation(len(cfgs))
+        te = np.sort(perm[: len(cfgs) // 5])
+        np.savez_compressed(os.path.join(out_dir, "picker_dataset.npz"), X=X, T=T.astype(np.float32), Lb=Lb,
+                            valid=valid, test=te, configs=json.dumps(cfgs))
+    t_measure = time.time() - t0
+    tr = np.setdiff1d(np.arange(len(cfgs)), te)
+    Y, M, st = pk.targets(T[tr], Lb[tr], valid[tr])
+    t1 = time.time()
+    mlp, losses = pk.train(X[tr], Y, M, steps=args.picker_steps, log=log)
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    pred = pk.predict(mlp, X[te])
+    ev = pk.evaluate(pred, T[te], Lb[te], valid[te], [cfgs[i] for i in te])
+    # Pick latency: one forward pass of a 16-row batch, device-timed.
+    x16 = torch.from_numpy(X[:16].copy() if len(X) >= 16 else np.zeros((16, pk.IN_DIM), np.float32)).cuda()
+    for _ in range(5):
+        mlp.forward(x16)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(100):
+        mlp.forward(x16)
+    e1.record()
+    torch.cuda.synchronize()
+    meta = {"calls": len(cfgs), "held_out": int(len(te)), "train_steps": args.picker_steps,
+            "device": torch.cuda.get_device_name(0)}
+    pk.save(os.path.join(out_dir, "picker_weights.npz"), mlp, st, meta)
+    line = {"suite": "picker", "metric": "learned pick vs exhaustive search (held-out calls)",
+            **ev, "calls_measured": len(cfgs), "arms": pk.NARMS,
+            "valid_arms_per_call_mean": float(valid.sum(1).mean()) if len(cfgs) else 0.0,
+            "train_loss_first_last": [losses[0], float(np.mean(losses[-50:]))],
+            "measure_s": t_measure, "train_s": t_train, "forward16_us": e0.elapsed_time(e1) * 10.0,
+            "config": {"model": "bine_mlp 16-256-256-256-%d GELU, bf16 weights, fp32 accumulate" % pk.OUT_DIM,
+                       "engine": "steps", "timing": "median of 3 CUDA-event launches per arm",
+                       "calls": "sampled: 60% allreduce / 20% reduce_scatter / 20% allgather, P on [4, 4096], "
+                                "per-rank message log-uniform 32 B..256 MiB (P x message <= 2 GiB)"}}
+    print(json.dumps(line))
+    return 0
 
 
 def main():
@@ -481,12 +579,20 @@ def main():
     ap.add_argument("--dtype", default="int32", choices=["int32", "float"])
     ap.add_argument("--engine", default="fused", choices=["fused", "steps"])
     ap.add_argument("--order", default="reference", choices=["reference", "fast"])
-    ap.add_argument("--suite", default="headline", choices=["headline", "batch"])
+    ap.add_argument("--suite", default="headline", choices=["headline", "batch", "picker"])
     ap.add_argument("--batch-n", type=int, default=4096)
+    ap.add_argument("--picker-n", type=int, default=1500)
+    ap.add_argument("--picker-seed", type=int, default=11)
+    ap.add_argument("--picker-budget", type=float, default=900.0, help="seconds of measurement at most")
+    ap.add_argument("--picker-steps", type=int, default=4000)
+    ap.add_argument("--picker-data", default=None, help="a measured picker_dataset.npz to train on")
+    ap.add_argument("--out", default=None, help="directory for the picker's dataset and weights")
     args = ap.parse_args()
     configure(args)
     if args.suite == "batch":
         return run_batch_suite(args)
+    if args.suite == "picker":
+        return run_picker_suite(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -110,6 +110,7 @@ def lib():
         "bine_comm_set_float_order": [vp, i],
         "bine_comm_set_step_timeout": [vp, ctypes.c_uint],
         "bine_debug_set_barrier_extra": [vp, ctypes.c_uint],
+        "bine_comm_set_tree_split": [vp, ctypes.c_int],
         "bine_comm_synchronize": [vp],
         "bine_allreduce": [vp, vp, i, i, i, vp],
         "bine_reduce_scatter": [vp, vp, ctypes.POINTER(ci), i, i, vp],
@@ -232,6 +233,11 @@ class Comm:
 
     def set_step_timeout(self, ms):
         check(lib().bine_comm_set_step_timeout(self._h, ms))
+
+    def set_tree_split(self, lanes):
+        """Lanes per output vector of the exact-order float reduction
+        (0: chosen per call)."""
+        check(lib().bine_comm_set_tree_split(self._h, lanes))
 
     def debug_set_barrier_extra(self, extra):
         check(lib().bine_debug_set_barrier_extra(self._h, extra))
@@ -406,6 +412,20 @@ class Batch:
         return best, ms.value
 
 
+def mlp_layout(in_dim, hidden, out_dim):
+    """Parameter arena of bine_mlp: per layer (weight offset, bias offset,
+    out, in); weights row-major [out, in], every block padded to 16 floats."""
+    dims = [in_dim, hidden, hidden, hidden, out_dim]
+    off, out = 0, []
+    for l in range(4):
+        w = off
+        off = (off + dims[l] * dims[l + 1] + 15) // 16 * 16
+        b = off
+        off = (off + dims[l + 1] + 15) // 16 * 16
+        out.append((w, b, dims[l + 1], dims[l]))
+    return out
+
+
 class MLP:
     """bine_mlp_*: in -> H -> H -> H -> out MLP (GELU, bf16 weights and
     activations, fp32 accumulation) trained with the engine's own kernels."""
@@ -425,16 +445,7 @@ class MLP:
 
     def layout(self):
         """(weight offset, bias offset, out, in) per layer in the parameter arena."""
-        din, h, dout = self.dims
-        dims = [din, h, h, h, dout]
-        off, out = 0, []
-        for l in range(4):
-            w = off
-            off = (off + dims[l] * dims[l + 1] + 15) // 16 * 16
-            b = off
-            off = (off + dims[l + 1] + 15) // 16 * 16
-            out.append((w, b, dims[l + 1], dims[l]))
-        return out
+        return mlp_layout(*self.dims)
 
     def get_params(self):
         out = np.zeros(self.nparams, np.float32)

@@ -1,0 +1,429 @@
+"""Learned variant picker for the step engine.
+
+For each call it picks the schedule the STEPS engine runs: the Bine variant
+(for allreduce the latency-optimal tree "L" against the bandwidth-optimal
+reduce-scatter + allgather "B", "B_COALESCE", "B_CONT"), the port count
+and the segment size (the engine's unit of work per block).  These are the
+choices the reference leaves to LIBBINE_* variables and its sweep scripts.
+None of them changes a result: they only change time.
+
+* Features (one row per call): op one-hot, log2 P, log2 message bytes,
+  torus shape (number of dimensions and log2 of each), dtype one-hot.
+* Targets per arm: log2 measured GPU time and log2 of the busiest torus
+  link's bytes, both generated by this engine (bench.py --suite picker).
+* Model: bine_mlp (3 x 256, GELU, bf16 weights, fp32 accumulation),
+  trained on the GPU with the engine's own kernels.
+* Judge: exhaustive search (every valid arm measured).  Fallback: the
+  reference's fixed rule (fixed_rule below), used when no model is loaded
+  or the model's pick is not valid for the call.
+"""
+import json
+import math
+import os
+
+import numpy as np
+
+# --------------------------------------------------------------- arm space
+SEGMENTS = [0, 4096, 65536]  # LIBBINE_SEGMENT_SIZE values the reference sweeps (0: engine default)
+PORTS = [1, 2, 6]
+ARMS = []
+for v in ["L", "B", "B_COALESCE", "B_CONT"]:
+    for p in PORTS:
+        for s in SEGMENTS:
+            ARMS.append(("allreduce", v, p, s))
+for s in SEGMENTS:
+    ARMS.append(("reduce_scatter", "VEC_HALVING_CONT_PERMUTE", 1, s))
+for v in ["VEC_DOUBLING_CONT_PERMUTE", "VEC_DOUBLING_CONT_SEND", "VEC_DOUBLING_BLOCKS"]:
+    for p in PORTS:
+        for s in SEGMENTS:
+            ARMS.append(("allgather", v, p, s))
+NARMS = len(ARMS)
+IN_DIM = 16
+OUT_DIM = ((2 * NARMS + 15) // 16) * 16
+OPS = ["allreduce", "reduce_scatter", "allgather"]
+# Planning the per-block B schedules costs O(P^2 * ports) on the host; arms
+# beyond these sizes are not offered.
+MAX_P = {"B": 128, "B_COALESCE": 256}
+
+
+def is_p2(x):
+    return x > 0 and (x & (x - 1)) == 0
+
+
+def message_bytes(coll, P, count, es):
+    """Per-rank message: the larger per-rank buffer."""
+    if coll == "allreduce":
+        return count * es
+    return count * es * P  # reduce_scatter send row / allgather receive row
+
+
+def features(coll, P, count, es, dims=None):
+    dims = list(dims or [P])
+    f = np.zeros(IN_DIM, np.float32)
+    f[OPS.index(coll)] = 1.0
+    f[3] = math.log2(P) / 12.0
+    f[4] = math.log2(max(1, message_bytes(coll, P, count, es))) / 28.0
+    f[5] = len(dims) / 3.0
+    for i, d in enumerate(dims[:3]):
+        f[6 + i] = math.log2(d) / 12.0
+    f[9] = 1.0 if es == 4 else 0.0
+    f[10] = 1.0 if es != 4 else 0.0
+    f[11] = 1.0 if is_p2(P) else 0.0
+    f[12] = math.log2(max(1, count)) / 28.0
+    return f
+
+
+def statically_valid(arm, coll, P, count, dims=None):
+    """Arms the engine can plan for this call (the planner has the final
+    word: cases it rejects are invalid too)."""
+    c, v, ports, seg = arm
+    if c != coll:
+        return False
+    if coll == "allreduce":
+        if v in MAX_P and P > MAX_P[v]:
+            return False
+        if v == "B_CONT" and not is_p2(P):
+            return False
+        if v != "L" and count < ports * P:
+            return False
+        if v == "L" and count < ports:
+            return False
+        return True
+    if coll == "reduce_scatter":
+        return is_p2(P)
+    if coll == "allgather":
+        if v in ("VEC_DOUBLING_CONT_PERMUTE", "VEC_DOUBLING_CONT_SEND") and not is_p2(P):
+            return False
+        if v == "VEC_DOUBLING_CONT_SEND" and ports != 1:
+            return False
+        if v == "VEC_DOUBLING_BLOCKS" and ports != 1:
+            return False  # the block-by-block allgather ignores LIBBINE_NUM_PORTS
+        return count >= ports
+    return False
+
+
+def fixed_rule(coll, P, count, es):
+    """The reference's own selection, composed from its defaults and sweep
+    scripts: variant B (lib/libbine.cc:56) when count >= ports*P
+    (lib/libbine.cc:1036), else L; ports 1 up to 128 KiB per rank, else 6
+    (bench/run_allreduce.sh:21-31); segment 0 up to 16 KiB, 4 KiB up to
+    128 KiB, else 64 KiB (bench/run_allreduce.sh:3-17).  Per-block B beyond
+    the planning cap becomes B_COALESCE (the same data movement, coalesced);
+    reduce_scatter keeps its single variant; allgather keeps its default
+    CONT_PERMUTE where it runs and the block-by-block variant elsewhere."""
+    msg = message_bytes(coll, P, count, es)
+    ports = 1 if msg <= 128 * 1024 else 6
+    seg = 0 if msg <= 16 * 1024 else (4096 if msg <= 128 * 1024 else 65536)
+    if coll == "allreduce":
+        while ports > 1 and count < ports:
+            ports = 2 if ports == 6 else 1
+        if count >= ports * P:
+            v = "B" if P <= MAX_P["B"] else "B_COALESCE"
+            if v == "B_COALESCE" and P > MAX_P["B_COALESCE"]:
+                v = "B_CONT" if is_p2(P) else "L"
+        else:
+            v = "L"
+        if v == "L":
+            while ports > 1 and count < ports:
+                ports = 2 if ports == 6 else 1
+        arm = ("allreduce", v, ports, seg)
+    elif coll == "reduce_scatter":
+        arm = ("reduce_scatter", "VEC_HALVING_CONT_PERMUTE", 1, seg)
+    else:
+        v = "VEC_DOUBLING_CONT_PERMUTE" if is_p2(P) else "VEC_DOUBLING_BLOCKS"
+        if v == "VEC_DOUBLING_BLOCKS":
+            ports = 1
+        while ports > 1 and count < ports:
+            ports = 2 if ports == 6 else 1
+        arm = ("allgather", v, ports, seg)
+    return ARMS.index(arm)
+
+
+def apply_arm(comm, arm):
+    coll, v, ports, seg = arm
+    comm.set_algo(coll, v)
+    comm.set_ports(ports)
+    comm.set_segment(seg)
+
+
+# ------------------------------------------------------------ data sampling
+P_GRID = sorted({int(round(2 ** (k / 4.0))) for k in range(8, 49)} | {6, 12, 24, 48, 96, 384})
+# reduce_scatter / allgather schedules move every block separately
+# (P^2 log P moves); planning beyond 1024 ranks takes tens of seconds.
+MAX_P_VECTOR = 1024
+
+
+def sample_configs(n, seed, max_total_bytes=2 << 30):
+    """Calls: op 60/20/20 allreduce/reduce_scatter/allgather, P log-uniform
+    on a grid over [4, 4096] ([4, 1024] for the vector collectives),
+    per-rank message log-uniform 32 B..256 MiB (capped so P x message <=
+    max_total_bytes), int32 or float32, one in three on a 2-D or 3-D torus
+    when P is a power of two >= 16."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        coll = str(rng.choice(OPS, p=[0.6, 0.2, 0.2]))
+        grid = P_GRID if coll == "allreduce" else [p for p in P_GRID if p <= MAX_P_VECTOR]
+        P = int(rng.choice(grid))
+        es = 4
+        dt = "int32" if rng.random() < 0.5 else "float"
+        m = 32 * 2 ** (rng.random() * 23)
+        m = min(m, max_total_bytes / P)
+        count = max(1, int(m // es)) if coll == "allreduce" else max(1, int(m // (es * P)))
+        dims = [P]
+        if is_p2(P) and P >= 16 and rng.random() < 1 / 3:
+            k = int(math.log2(P))
+            if rng.random() < 0.5:
+                a = k // 2
+                dims = [2 ** a, 2 ** (k - a)]
+            else:
+                a = k // 3
+                b = (k - a) // 2
+                dims = [2 ** a, 2 ** b, 2 ** (k - a - b)]
+        out.append({"coll": coll, "P": P, "count": count, "es": es, "dtype": dt, "dims": dims})
+    return out
+
+
+def measure(configs, reps=3, time_budget_s=None, log=None):
+    """Measures every valid arm of every call on the GPU with the STEPS
+    engine: median of `reps` launches timed with CUDA events, and the
+    busiest link's bytes from the engine's device link accounting.  Calls
+    are grouped by torus so each communicator (and its proof cache) serves
+    many calls.  Returns (configs measured, X [n, IN_DIM], T_us [n, NARMS],
+    L_bytes [n, NARMS], valid [n, NARMS]); arms the engine refuses are
+    invalid.  Stops early, keeping whole calls, once time_budget_s passes."""
+    import time
+
+    import torch
+
+    import bine_trees_fugaku_b200 as bine
+
+    stream = torch.cuda.current_stream()
+    keys = sorted({(c["P"], tuple(c["dims"])) for c in configs})
+    perm = np.random.default_rng(0).permutation(len(keys))  # a budget stop keeps every P range
+    group = {k: int(perm[j]) for j, k in enumerate(keys)}
+    order = sorted(range(len(configs)), key=lambda i: (group[(configs[i]["P"], tuple(configs[i]["dims"]))], i))
+    cfgs, X, T, Lb = [], [], [], []
+    t_start = time.time()
+    comm, comm_key = None, None
+    for i in order:
+        if time_budget_s and time.time() - t_start > time_budget_s:
+            break
+        cfg = configs[i]
+        coll, P, count, es, dims = cfg["coll"], cfg["P"], cfg["count"], cfg["es"], cfg["dims"]
+        if (P, tuple(dims)) != comm_key:
+            if comm is not None:
+                comm.close()
+            comm = bine.Comm(P, dims if len(dims) > 1 else None)
+            comm.set_engine("steps")
+            comm.set_stream(stream)
+            comm_key = (P, tuple(dims))
+        se, re = bine.row_counts(coll, count, P)
+        dtype = torch.int32 if cfg["dtype"] == "int32" else torch.float32
+        code = bine.INT32 if cfg["dtype"] == "int32" else bine.FLOAT
+        send = torch.ones((P, se), dtype=dtype, device="cuda")
+        recv = torch.zeros((P, re), dtype=dtype, device="cuda")
+        links = torch.zeros(P * len(dims) * 2, dtype=torch.int64, device="cuda")
+        t_row = np.full(NARMS, np.nan)
+        l_row = np.full(NARMS, np.nan)
+        for a, arm in enumerate(ARMS):
+            if not statically_valid(arm, coll, P, count, dims):
+                continue
+            try:
+                apply_arm(comm, arm)
+                comm.run(coll, send, recv, count, code)  # plans, proves and uploads once
+                comm.synchronize()
+            except bine.BineError:
+                continue
+            ts = []
+            for _ in range(reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                comm.run(coll, send, recv, count, code)
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1) * 1e3)
+            comm.synchronize()
+            t_row[a] = float(np.median(ts))
+            comm.link_bytes(coll, count, code, links)
+            l_row[a] = float(links.max().item())
+        del send, recv, links
+        cfgs.append(cfg)
+        X.append(features(coll, P, count, es, dims))
+        T.append(t_row)
+        Lb.append(l_row)
+        if log and len(cfgs) % 50 == 0:
+            log(f"measured {len(cfgs)}/{len(configs)} calls in {time.time() - t_start:.0f} s (P={P})")
+    if comm is not None:
+        comm.close()
+    T = np.array(T).reshape(-1, NARMS)
+    Lb = np.array(Lb).reshape(-1, NARMS)
+    return cfgs, np.array(X, np.float32).reshape(-1, IN_DIM), T, Lb, ~np.isnan(T)
+
+
+# ------------------------------------------------------------- the model
+def targets(T, Lb, valid):
+    """Standardised log2 targets; returns (Y [n, OUT_DIM], mask, stats)."""
+    n = T.shape[0]
+    lt = np.where(valid, np.log2(np.maximum(T, 1e-3)), 0.0)
+    ll = np.where(valid, np.log2(np.maximum(Lb, 0.0) + 1.0), 0.0)
+    st = {"t_mean": float(lt[valid].mean()), "t_std": float(lt[valid].std() + 1e-9),
+          "l_mean": float(ll[valid].mean()), "l_std": float(ll[valid].std() + 1e-9)}
+    Y = np.zeros((n, OUT_DIM), np.float32)
+    M = np.zeros((n, OUT_DIM), np.float32)
+    Y[:, :NARMS] = (lt - st["t_mean"]) / st["t_std"]
+    Y[:, NARMS:2 * NARMS] = (ll - st["l_mean"]) / st["l_std"]
+    M[:, :NARMS] = valid
+    M[:, NARMS:2 * NARMS] = valid
+    return Y, M, st
+
+
+def train(X, Y, M, steps=3000, batch=256, lr=1e-3, seed=0, log=None):
+    """Trains bine_mlp on the GPU; returns (mlp, losses)."""
+    import torch
+
+    import bine_trees_fugaku_b200 as bine
+
+    mlp = bine.MLP(IN_DIM, 256, OUT_DIM, batch, seed=seed)
+    rng = np.random.default_rng(seed)
+    n = X.shape[0]
+    Xd, Yd, Md = (torch.from_numpy(a).cuda() for a in (X, Y, M))
+    losses = []
+    for s in range(steps):
+        idx = torch.from_numpy(rng.integers(0, n, batch)).cuda()
+        cur = lr * 0.5 * (1 + math.cos(math.pi * s / steps))
+        loss = mlp.train_step(Xd[idx].contiguous(), Yd[idx].contiguous(), Md[idx].contiguous(), cur)
+        losses.append(loss)
+        if log and s % 500 == 0:
+            log(f"step {s} loss {loss:.4f}")
+    return mlp, losses
+
+
+def predict(mlp, X):
+    """Model outputs [n, OUT_DIM] (standardised log2 time, log2 link bytes)."""
+    import torch
+
+    n = X.shape[0]
+    pad = (-n) % 16
+    Xp = np.concatenate([X, np.zeros((pad, IN_DIM), np.float32)]) if pad else X
+    out = []
+    bs = mlp.max_batch
+    for lo in range(0, Xp.shape[0], bs):
+        out.append(mlp.forward(torch.from_numpy(Xp[lo:lo + bs]).cuda()).cpu().numpy())
+    return np.concatenate(out)[:n]
+
+
+def evaluate(pred, T, Lb, valid, configs):
+    """Learned picks against exhaustive search (the measured optimum over
+    every valid arm) and against the fixed rule, on held-out calls.
+
+    Time objective: the arm with the lowest predicted time; its measured
+    time over the optimum's.  Link objective: the arm with the lowest
+    predicted busiest-link bytes; its bytes over the minimum."""
+    rows, within, ratio, speed, fixed_within, fixed_invalid = 0, 0, [], [], 0, 0
+    link_exact, link_ratio = 0, []
+    for i in range(T.shape[0]):
+        v = valid[i]
+        if not v.any():
+            continue
+        rows += 1
+        a = int(np.argmin(np.where(v, pred[i, :NARMS], np.inf)))
+        t_opt = float(np.min(T[i, v]))
+        within += T[i, a] <= 1.05 * t_opt
+        ratio.append(T[i, a] / t_opt)
+        c = configs[i]
+        fa = fixed_rule(c["coll"], c["P"], c["count"], c["es"])
+        if v[fa]:
+            speed.append(T[i, fa] / T[i, a])
+            fixed_within += T[i, fa] <= 1.05 * t_opt
+        else:
+            fixed_invalid += 1
+        al = int(np.argmin(np.where(v, pred[i, NARMS:2 * NARMS], np.inf)))
+        l_opt = float(np.min(Lb[i, v]))
+        link_exact += Lb[i, al] <= l_opt
+        link_ratio.append((Lb[i, al] + 1) / (l_opt + 1))
+    gm = lambda x: float(np.exp(np.mean(np.log(x)))) if x else None
+    return {"held_out_calls": rows,
+            "pick_within_5pct_of_optimum": within / max(1, rows),
+            "pick_time_over_optimum_geomean": gm(ratio),
+            "pick_time_over_optimum_max": float(max(ratio)) if ratio else None,
+            "fixed_rule_within_5pct_of_optimum": fixed_within / max(1, rows - fixed_invalid),
+            "speedup_vs_fixed_rule_geomean": gm(speed),
+            "calls_where_fixed_rule_is_refused": fixed_invalid,
+            "link_pick_is_minimum": link_exact / max(1, rows),
+            "link_bytes_over_minimum_geomean": gm(link_ratio)}
+
+
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "picker_weights.npz")
+
+
+def save(path, mlp, stats, meta):
+    """Saves the weights as the bf16 values the forward pass uses (the
+    master copies are fp32; forward rounds them to bf16)."""
+    p = mlp.get_params()
+    bits = (p.view(np.uint32) + 0x7FFF + ((p.view(np.uint32) >> 16) & 1)) >> 16  # round to nearest even
+    np.savez_compressed(path, params_bf16=bits.astype(np.uint16), stats=json.dumps(stats),
+                        meta=json.dumps(meta), arms=json.dumps(ARMS), dims=np.array([IN_DIM, 256, OUT_DIM]))
+
+
+def load_params(path):
+    """(params as float32, dims, stats, meta) of a saved picker."""
+    z = np.load(path)
+    p = (z["params_bf16"].astype(np.uint32) << 16).view(np.float32)
+    return p, tuple(int(v) for v in z["dims"]), json.loads(str(z["stats"])), json.loads(str(z["meta"])), \
+        json.loads(str(z["arms"]))
+
+
+class Picker:
+    """Runtime picker.  With trained weights it ranks the arms by predicted
+    time (bine_mlp forward on the GPU) and takes the first one the planner
+    proves correct for the call; without weights it takes the fixed rule,
+    then the latency-optimal tree (allreduce) or the block-by-block
+    allgather when the planner refuses the rule's arm.  Picks are cached
+    per call shape."""
+
+    def __init__(self, path=DEFAULT_WEIGHTS):
+        import bine_trees_fugaku_b200 as bine
+
+        self.mlp = None
+        self.cache = {}
+        if path and os.path.exists(path):
+            p, dims, _, _, arms = load_params(path)
+            if [tuple(a) for a in arms] != ARMS or dims != (IN_DIM, 256, OUT_DIM):
+                raise ValueError(f"{path}: arm space or model shape differs from this build")
+            self.mlp = bine.MLP(dims[0], dims[1], dims[2], 16, seed=0)
+            self.mlp.set_params(p)
+
+    def ranking(self, coll, P, count, es, dims=None):
+        """Candidate arm indices, best first."""
+        ok = [a for a, arm in enumerate(ARMS) if statically_valid(arm, coll, P, count, dims)]
+        if self.mlp is None or not ok:
+            first = fixed_rule(coll, P, count, es)
+            rest = [a for a in ok if ARMS[a][1] in ("L", "VEC_DOUBLING_BLOCKS") and a != first]
+            return [first] + rest
+        x = np.zeros((16, IN_DIM), np.float32)
+        x[0] = features(coll, P, count, es, dims)
+        t = predict(self.mlp, x)[0, :NARMS]
+        return sorted(ok, key=lambda a: t[a])
+
+    def choose(self, comm, coll, count, es):
+        """Applies the best provable arm to `comm` and returns it."""
+        import bine_trees_fugaku_b200 as bine
+
+        key = (coll, comm.nranks, tuple(comm.dims), count, es)
+        if key not in self.cache:
+            self.cache[key] = None
+            for a in self.ranking(coll, comm.nranks, count, es, comm.dims):
+                apply_arm(comm, ARMS[a])
+                try:
+                    comm.plan_verify(coll, count)
+                except bine.Unsupported:
+                    continue
+                self.cache[key] = a
+                break
+        a = self.cache[key]
+        if a is None:
+            raise bine.Unsupported(bine.ERR_UNSUPPORTED, f"no Bine schedule runs {coll} at P={comm.nranks}")
+        apply_arm(comm, ARMS[a])
+        return ARMS[a]
