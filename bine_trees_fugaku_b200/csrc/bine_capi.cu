@@ -81,10 +81,25 @@ struct DevTrees {
     int ntiles = 0;
     int max_prog_len = 0;
     bool vec_ok = false;  // every offset and shift is a multiple of 16 bytes
+    // Split form (k_tree_split), used when split_k > 1 and the layout is
+    // 16-byte aligned: the same segments over the split programs.
+    int split_k = 1;
+    dev::TreeSeg* ssegs = nullptr;
+    dev::TreeEntry* sprog = nullptr;
+    int* sparts = nullptr;
+    dev::TreeComb* scomb = nullptr;
+    dev::TreeTile* stiles = nullptr;
+    int nstiles = 0;
+    int smax_prog_len = 0;
     ~DevTrees() {
         cudaFree(segs);
         cudaFree(prog);
         cudaFree(tiles);
+        cudaFree(ssegs);
+        cudaFree(sprog);
+        cudaFree(sparts);
+        cudaFree(scomb);
+        cudaFree(stiles);
     }
 };
 
@@ -136,6 +151,8 @@ struct bine_comm_s {
     std::unordered_map<StructKey, int, StructKeyHash> verified;  // 1: proven, 0: refuted
     std::unordered_map<StructKey, std::string, StructKeyHash> refuted_why;
     long long segment_bytes = 0;
+    int64_t cached_moves = 0;  // moves held by `schedules`
+    int tree_split = 0;        // lanes per output vector in k_tree_split (0: chosen per call)
     // Device state, created on first use.
     int device = -1;
     int num_sms = 0;
@@ -166,6 +183,20 @@ PlanKey make_key(bine_comm_t c, int coll, long count, int root) {
     return k;
 }
 
+// Plan caches hold one entry per distinct call (count included); a caller
+// that sweeps many counts would otherwise grow host and device memory
+// without bound.  A full cache is emptied before the next insertion;
+// entries a launch is still reading stay alive through its shared_ptr, and
+// cudaFree in their destructors waits for kernels in flight.
+constexpr size_t kMaxCachedSchedules = 64;
+constexpr int64_t kMaxCachedMoves = 32ll << 20;  // ~2 GB of host schedule moves
+constexpr size_t kMaxCachedDeviceTables = 64;
+
+template <typename Map>
+void trim(Map& m, size_t limit) {
+    if (m.size() >= limit) m.clear();
+}
+
 int get_schedule(bine_comm_t c, const PlanKey& k, std::shared_ptr<Schedule>* out) {
     std::lock_guard<std::mutex> lk(c->mu);
     auto it = c->schedules.find(k);
@@ -176,6 +207,13 @@ int get_schedule(bine_comm_t c, const PlanKey& k, std::shared_ptr<Schedule>* out
     auto s = std::make_shared<Schedule>();
     std::string err;
     if (!c->planner->build(k, s.get(), &err)) return fail(BINE_ERR_UNSUPPORTED, err);
+    int64_t moves = 0;
+    for (const auto& lvl : s->levels) moves += (int64_t)lvl.size();
+    if (c->schedules.size() >= kMaxCachedSchedules || c->cached_moves + moves > kMaxCachedMoves) {
+        c->schedules.clear();
+        c->cached_moves = 0;
+    }
+    c->cached_moves += moves;
     c->schedules.emplace(k, s);
     *out = s;
     return BINE_SUCCESS;
@@ -294,6 +332,7 @@ int get_dev_steps(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSt
     fill(&d->level_begin, lb, &e3);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
         return fail(BINE_ERR_CUDA, "uploading the schedule failed");
+    trim(c->dev_steps, kMaxCachedDeviceTables);
     c->dev_steps.emplace(key, d);
     *out = d;
     return BINE_SUCCESS;
@@ -304,7 +343,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
     int rc = get_schedule(c, k, &s);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
-    PlanKeyEs key{k, es, 0};
+    PlanKeyEs key{k, es, c->tree_split};
     auto it = c->dev_trees.find(key);
     if (it != c->dev_trees.end()) {
         *out = it->second;
@@ -351,6 +390,58 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
     fill(&d->tiles, tiles, &e3);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
         return fail(BINE_ERR_CUDA, "uploading the reduction trees failed");
+    // Split form: K lanes per output vector when the output has too few
+    // vectors to fill the GPU several times over (the last wave of a
+    // one-vector-per-thread launch would run mostly empty).
+    if (vec) {
+        int min_leaves = INT32_MAX;
+        long long vecs = 0;
+        for (const OutSegment& sg : tp.segs) {
+            min_leaves = std::min(min_leaves, sg.prog_len);  // one leaf per program entry
+            vecs += sg.n / (16 / es);
+        }
+        int K = 1;
+        if (c->tree_split > 0) {
+            K = c->tree_split;
+            while (K > 1 && min_leaves < K) K /= 2;
+        } else {
+            const long long resident_threads = (long long)std::max(1, c->num_sms) * 2048;
+            while (K < 8 && vecs * K < 8 * resident_threads && min_leaves >= 16 * K * 2) K *= 2;
+        }
+        if (K > 1) {
+            SplitTrees st;
+            if (!split_trees(tp, K, &st, &err)) return fail(BINE_ERR_INTERNAL, err);
+            if (st.max_depth > dev::kMaxTreeDepth) return fail(BINE_ERR_UNSUPPORTED, "reduction tree deeper than supported");
+            std::vector<dev::TreeSeg> ssegs;
+            std::vector<int> sparts;
+            std::vector<dev::TreeComb> scomb;
+            std::vector<dev::TreeTile> stiles;
+            for (size_t i = 0; i < tp.segs.size(); i++) {
+                const OutSegment& sg = tp.segs[i];
+                const int32_t b = st.parts[i * (K + 1)], e = st.parts[i * (K + 1) + K];
+                ssegs.push_back(dev::TreeSeg{sg.off, sg.n, sg.rank, b, e - b, sg.depth});
+                d->smax_prog_len = std::max(d->smax_prog_len, e - b);
+                for (int j = 0; j <= K; j++) sparts.push_back(st.parts[i * (K + 1) + j] - b);
+                for (int j = 0; j < K; j++) scomb.push_back(dev::TreeComb{st.comb[i * K + j].first, st.comb[i * K + j].second});
+                const int64_t stile = (int64_t)(dev::kThreads / K) * (16 / es);
+                for (int64_t s0 = 0; s0 < sg.n; s0 += stile)
+                    stiles.push_back(dev::TreeTile{(int32_t)i, 0, s0, std::min(stile, sg.n - s0)});
+            }
+            std::vector<dev::TreeEntry> sprog;
+            for (const ProgEntry& e : st.prog) sprog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
+            cudaError_t f1, f2, f3, f4, f5;
+            fill(&d->ssegs, ssegs, &f1);
+            fill(&d->sprog, sprog, &f2);
+            fill(&d->sparts, sparts, &f3);
+            fill(&d->scomb, scomb, &f4);
+            fill(&d->stiles, stiles, &f5);
+            if (f1 != cudaSuccess || f2 != cudaSuccess || f3 != cudaSuccess || f4 != cudaSuccess || f5 != cudaSuccess)
+                return fail(BINE_ERR_CUDA, "uploading the split reduction trees failed");
+            d->nstiles = (int)stiles.size();
+            d->split_k = K;
+        }
+    }
+    trim(c->dev_trees, kMaxCachedDeviceTables);
     c->dev_trees.emplace(key, d);
     *out = d;
     return BINE_SUCCESS;
@@ -424,11 +515,36 @@ int launch_sum_dt(bine_comm_t c, int dt, int mode, const char* in, long long ist
     return fail(BINE_ERR_ARG, "bad datatype");
 }
 
+template <typename T, int K>
+int launch_tree_split(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost) {
+    const size_t smem = (size_t)d.smax_prog_len * sizeof(dev::TreeEntry);
+    auto kern = dev::k_tree_split<T, K>;
+    if (smem > 200 * 1024) return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
+    if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, dev::kThreads, smem));
+    // One resident wave of blocks walking the tiles: consecutive tiles of a
+    // block share a segment, so its program is staged once.
+    const long long resident = (long long)std::max(1, per_sm) * std::max(1, c->num_sms);
+    const unsigned g = (unsigned)std::max(1LL, std::min<long long>(d.nstiles, resident));
+    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.ssegs, d.sprog, d.sparts, d.scomb, d.stiles,
+                                                d.nstiles);
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
 template <typename T>
 int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost) {
     if (d.ntiles == 0) return BINE_SUCCESS;
     const size_t smem = (size_t)d.max_prog_len * sizeof(dev::TreeEntry);
     const bool vec = d.vec_ok && aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0;
+    if (vec && d.split_k > 1) {
+        switch (d.split_k) {
+        case 2: return launch_tree_split<T, 2>(c, d, in, ist, out, ost);
+        case 4: return launch_tree_split<T, 4>(c, d, in, ist, out, ost);
+        case 8: return launch_tree_split<T, 8>(c, d, in, ist, out, ost);
+        }
+    }
     auto kern = vec ? dev::k_tree_vec<T> : dev::k_tree_scalar<T>;
     if (smem > 227 * 1024) return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
     if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1097,6 +1213,14 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms) {
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     comm->barrier_extra = extra;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_tree_split(bine_comm_t comm, int lanes) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (lanes != 0 && lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8)
+        return fail(BINE_ERR_ARG, "tree split must be 0, 1, 2, 4 or 8");
+    comm->tree_split = lanes;
     return BINE_SUCCESS;
 }
 

@@ -277,6 +277,103 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
     }
 }
 
+// Split form of k_tree_vec.  Each output vector is evaluated by a group of
+// K lanes of one warp: the host cut every segment's tree into K disjoint
+// subtrees (the "parts", in left-to-right order) and a combine program whose
+// leaves are the parts.  Lane j evaluates part j; the group exchanges the K
+// partial sums by shuffles and every lane runs the combine program, so the
+// additions and their association are exactly the tree's.  K times more,
+// K times shorter tasks remove the tail of the last wave when the output has
+// few vectors per resident thread.  Lanes then share the P output stores.
+struct TreeComb {  // combine entry: push part `part`, then `adds` additions
+    int32_t part, adds;
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict__ in, long long in_stride,
+                                                         char* __restrict__ out, long long out_stride, int P,
+                                                         const TreeSeg* __restrict__ segs,
+                                                         const TreeEntry* __restrict__ prog,
+                                                         const int* __restrict__ parts,
+                                                         const TreeComb* __restrict__ comb,
+                                                         const TreeTile* __restrict__ tiles, int ntiles) {
+    extern __shared__ TreeEntry sprog[];
+    __shared__ int spart[K + 1];
+    __shared__ TreeComb scomb[K];
+    constexpr int L = 16 / sizeof(T);
+    const int j = threadIdx.x % K;
+    const int gbase = (threadIdx.x & 31) & ~(K - 1);  // first lane of this group in the warp
+    int cur = -1;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const TreeTile tile = tiles[t];
+        const TreeSeg sg = segs[tile.seg];
+        if (tile.seg != cur) {  // block-uniform
+            __syncthreads();
+            for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
+            if (threadIdx.x <= K) spart[threadIdx.x] = parts[(long long)tile.seg * (K + 1) + threadIdx.x];
+            if (threadIdx.x < K) scomb[threadIdx.x] = comb[(long long)tile.seg * K + threadIdx.x];
+            __syncthreads();
+            cur = tile.seg;
+        }
+        const long long col = (long long)(threadIdx.x / K) * L;
+        const bool active = col < tile.n;
+        const long long e = sg.off + tile.start + col;
+        uint4 top = make_uint4(0, 0, 0, 0);
+        if (active) {
+            const int b = spart[j], len = spart[j + 1] - b;
+            uint4 stk[kMaxTreeDepth];
+            int sp = 0;
+            uint4 ring[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (u < len) {
+                    const TreeEntry q = sprog[b + u];
+                    ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                }
+            for (int k0 = 0; k0 < len; k0 += 4) {
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int k = k0 + u;
+                    if (k < len) {
+                        const uint4 v = ring[u];
+                        if (k + 4 < len) {
+                            const TreeEntry q = sprog[b + k + 4];
+                            ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                        }
+                        if (k > 0) stk[sp++] = top;
+                        top = v;
+                        for (int a = sprog[b + k].adds; a > 0; a--) top = vadd<T>(stk[--sp], top);
+                    }
+                }
+            }
+        }
+        // Every lane of the warp takes part in the exchange (inactive lanes
+        // carry zeros nobody reads).
+        const uint4 mine = top;
+        uint4 cstk[K];
+        int csp = 0;
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+            const TreeComb c = scomb[q];
+            const int src = gbase + c.part;
+            uint4 v;
+            v.x = __shfl_sync(0xffffffffu, mine.x, src);
+            v.y = __shfl_sync(0xffffffffu, mine.y, src);
+            v.z = __shfl_sync(0xffffffffu, mine.z, src);
+            v.w = __shfl_sync(0xffffffffu, mine.w, src);
+            if (q > 0) cstk[csp++] = top;
+            top = v;
+            for (int a = c.adds; a > 0; a--) top = vadd<T>(cstk[--csp], top);
+        }
+        if (!active) continue;
+        if (sg.rank < 0) {
+            for (int d = j; d < P; d += K) st_stream(out + (long long)d * out_stride + e * (long long)sizeof(T), top);
+        } else if (j == 0) {
+            st_stream(out + (long long)sg.rank * out_stride + e * (long long)sizeof(T), top);
+        }
+    }
+}
+
 // Element form for layouts that are not 16-byte aligned.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_tree_scalar(const char* __restrict__ in, long long in_stride,

@@ -1650,4 +1650,153 @@ bool link_bytes(const Torus& t, const std::vector<Message>& msgs, int es, std::v
     return true;
 }
 
+// ------------------------------------------------------------ tree split
+namespace {
+
+struct TNode {
+    int32_t l, r, leaves, entry;  // entry: index of the leaf's program entry (-1 for additions)
+};
+
+// Parses one postfix program into a binary tree; returns the root or -1.
+int parse_tree(const std::vector<ProgEntry>& prog, int begin, int len, std::vector<TNode>* nodes) {
+    std::vector<int> st;
+    for (int i = begin; i < begin + len; i++) {
+        nodes->push_back(TNode{-1, -1, 1, i});
+        st.push_back((int)nodes->size() - 1);
+        for (int a = 0; a < prog[i].adds; a++) {
+            if (st.size() < 2) return -1;
+            const int r = st.back();
+            st.pop_back();
+            const int l = st.back();
+            st.pop_back();
+            nodes->push_back(TNode{l, r, (*nodes)[l].leaves + (*nodes)[r].leaves, -1});
+            st.push_back((int)nodes->size() - 1);
+        }
+    }
+    return st.size() == 1 ? st[0] : -1;
+}
+
+// Postfix emission with the parse's child order (left subtree first), so
+// the evaluation order and stack depth of every subtree are unchanged.
+void emit_subtree(const std::vector<TNode>& nodes, const std::vector<ProgEntry>& prog, int n,
+                  std::vector<ProgEntry>* out) {
+    std::vector<std::pair<int, bool>> todo{{n, false}};
+    while (!todo.empty()) {
+        auto [x, expanded] = todo.back();
+        todo.pop_back();
+        const TNode& t = nodes[x];
+        if (t.entry >= 0) {
+            ProgEntry e = prog[t.entry];
+            e.adds = 0;
+            out->push_back(e);
+        } else if (expanded) {
+            out->back().adds++;
+        } else {
+            todo.push_back({x, true});
+            todo.push_back({t.r, false});
+            todo.push_back({t.l, false});
+        }
+    }
+}
+
+void emit_combine(const std::vector<TNode>& nodes, int n, const std::unordered_map<int, int>& part_of,
+                  std::vector<std::pair<int32_t, int32_t>>* out) {
+    std::vector<std::pair<int, bool>> todo{{n, false}};
+    while (!todo.empty()) {
+        auto [x, expanded] = todo.back();
+        todo.pop_back();
+        auto it = part_of.find(x);
+        if (it != part_of.end()) {
+            out->push_back({it->second, 0});
+        } else if (expanded) {
+            out->back().second++;
+        } else {
+            todo.push_back({x, true});
+            todo.push_back({nodes[x].r, false});
+            todo.push_back({nodes[x].l, false});
+        }
+    }
+}
+
+int stack_depth(const ProgEntry* p, int len) {
+    int sp = 0, mx = 0;
+    for (int i = 0; i < len; i++) {
+        mx = std::max(mx, ++sp);
+        sp -= p[i].adds;
+    }
+    return mx;
+}
+
+}  // namespace
+
+bool split_trees(const TreePlan& tp, int K, SplitTrees* out, std::string* err) {
+    out->K = K;
+    out->prog.clear();
+    out->parts.clear();
+    out->comb.clear();
+    out->max_depth = 0;
+    // Distinct programs are split once and shared by their segments.
+    std::map<std::pair<int32_t, int32_t>, std::pair<std::vector<int32_t>, std::vector<std::pair<int32_t, int32_t>>>>
+        done;
+    for (const OutSegment& sg : tp.segs) {
+        const auto key = std::make_pair(sg.prog_begin, sg.prog_len);
+        auto it = done.find(key);
+        if (it == done.end()) {
+            std::vector<TNode> nodes;
+            const int root = parse_tree(tp.prog, sg.prog_begin, sg.prog_len, &nodes);
+            if (root < 0) {
+                *err = "malformed reduction program";
+                return false;
+            }
+            // Cut the largest remaining subtree until there are K parts.
+            std::vector<int> fr{root};
+            while ((int)fr.size() < K) {
+                int best = -1;
+                for (int i = 0; i < (int)fr.size(); i++)
+                    if (nodes[fr[i]].entry < 0 && (best < 0 || nodes[fr[i]].leaves > nodes[fr[best]].leaves)) best = i;
+                if (best < 0) {
+                    *err = "reduction tree has fewer leaves than parts";
+                    return false;
+                }
+                const TNode t = nodes[fr[best]];
+                fr[best] = t.l;
+                fr.insert(fr.begin() + best + 1, t.r);
+            }
+            std::vector<int32_t> offs;
+            std::unordered_map<int, int> part_of;
+            for (int j = 0; j < K; j++) {
+                offs.push_back((int32_t)out->prog.size());
+                part_of[fr[j]] = j;
+                emit_subtree(nodes, tp.prog, fr[j], &out->prog);
+                out->max_depth = std::max(out->max_depth, stack_depth(out->prog.data() + offs.back(),
+                                                                      (int)out->prog.size() - offs.back()));
+            }
+            offs.push_back((int32_t)out->prog.size());
+            std::vector<std::pair<int32_t, int32_t>> comb;
+            emit_combine(nodes, root, part_of, &comb);
+            // Self-check: parts substituted into the combine program must
+            // reproduce the original program exactly.
+            std::vector<ProgEntry> back;
+            for (const auto& [j, adds] : comb) {
+                back.insert(back.end(), out->prog.begin() + offs[j], out->prog.begin() + offs[j + 1]);
+                back.back().adds += adds;
+            }
+            bool same = (int)back.size() == sg.prog_len && (int)comb.size() == K;
+            for (int i = 0; same && i < sg.prog_len; i++) {
+                const ProgEntry& a = back[i];
+                const ProgEntry& b = tp.prog[sg.prog_begin + i];
+                same = a.rank == b.rank && a.shift == b.shift && a.adds == b.adds;
+            }
+            if (!same) {
+                *err = "split reduction tree does not recompose to the original";
+                return false;
+            }
+            it = done.emplace(key, std::make_pair(offs, comb)).first;
+        }
+        out->parts.insert(out->parts.end(), it->second.first.begin(), it->second.first.end());
+        out->comb.insert(out->comb.end(), it->second.second.begin(), it->second.second.end());
+    }
+    return true;
+}
+
 }  // namespace bine

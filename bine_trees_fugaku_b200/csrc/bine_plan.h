@@ -123,6 +123,23 @@ struct TreePlan {
     int max_depth = 0;
 };
 
+// A TreePlan whose every program is cut into K disjoint subtrees ("parts",
+// left to right) plus a combine program over the parts, for evaluation by
+// K cooperating lanes.  Substituting each part for its combine leaf gives
+// back the original program entry for entry.
+struct SplitTrees {
+    int K = 1;
+    std::vector<ProgEntry> prog;  // the parts of every distinct program
+    // Per segment: K + 1 offsets into `prog` (part j is [parts[j], parts[j+1]))
+    std::vector<int32_t> parts;
+    // Per segment: K combine entries (part index, additions after it)
+    std::vector<std::pair<int32_t, int32_t>> comb;
+    int max_depth = 0;  // deepest evaluation stack of any part
+};
+
+// Returns false (with `err`) when some tree has fewer than K leaves.
+bool split_trees(const TreePlan& tp, int K, SplitTrees* out, std::string* err);
+
 class Planner {
   public:
     Planner(int nranks, int ndims, const int* dims);

@@ -200,6 +200,11 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms);
  * wait expires (0 restores normal operation).  Nothing faults or hangs. */
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
 
+/* Lanes that cooperate on one output vector in the exact-order float
+ * reduction (1, 2, 4 or 8; 0, the default, chooses per call from the
+ * output size).  Results are identical for every setting. */
+int bine_comm_set_tree_split(bine_comm_t comm, int lanes);
+
 /* ------------------------------------------------------------- batching
  * Many independent allreduce / reduce_scatter / allgather calls of
  * different rank counts, sizes and element types (BINE_INT32 or

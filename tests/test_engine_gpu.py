@@ -121,6 +121,31 @@ def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
     assert np.array_equal(out[rr].view(np.uint32), expect[rr].view(np.uint32))
 
 
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8])
+@pytest.mark.parametrize("coll,variant,P,count,dims,ports", [
+    ("allreduce", "B", 256, 256 * 64, None, 1),
+    ("allreduce", "B", 96, 96 * 512, None, 1),
+    ("allreduce", "B_COALESCE", 48, 48 * 776, None, 2),
+    ("allreduce", "L", 64, 50_000, None, 1),
+    ("allreduce", "L", 72, 30_000, [6, 12], 2),
+    ("allreduce", "B", 64, 64 * 600, [4, 4, 4], 6),
+    ("reduce_scatter", "VEC_HALVING_CONT_PERMUTE", 64, 1024, None, 1),
+    ("reduce", "BINOMIAL_TREE", 64, 20_000, None, 1),
+])
+def test_float_exact_order_split_lanes(lanes, coll, variant, P, count, dims, ports):
+    """The exact-order float kernel with every lane count per output vector
+    (the tree cut into 1, 2, 4 or 8 subtrees and recombined by shuffles)
+    returns the oracle's bits."""
+    sc, _ = buffer_counts(coll, count, P)
+    x = np.random.default_rng(P * 7 + count).standard_normal((P, sc)).astype(np.float32)
+    expect, _ = port.run(coll, x, count, variant=variant, dims=dims, ports=ports)
+    comm = make_comm(P, coll, variant, dims, ports)
+    comm.set_tree_split(lanes)
+    out = run(comm, coll, x, count)
+    rr = receiving_ranks(coll, P)
+    assert np.array_equal(out[rr].view(np.uint32), expect[rr].view(np.uint32))
+
+
 @pytest.mark.parametrize("coll", ["allgather", "bcast", "alltoall", "scatter", "gather"])
 @pytest.mark.parametrize("P,count,dt", [(64, 4096, np.float32), (32, 1001, np.int64), (16, 37, np.int8),
                                         (256, 1024, np.int32)])
