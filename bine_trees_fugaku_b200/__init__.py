@@ -111,6 +111,7 @@ def lib():
         "bine_comm_set_step_timeout": [vp, ctypes.c_uint],
         "bine_debug_set_barrier_extra": [vp, ctypes.c_uint],
         "bine_comm_set_tree_split": [vp, ctypes.c_int],
+        "bine_allreduce_host": [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp],
         "bine_comm_synchronize": [vp],
         "bine_allreduce": [vp, vp, i, i, i, vp],
         "bine_reduce_scatter": [vp, vp, ctypes.POINTER(ci), i, i, vp],
@@ -175,6 +176,15 @@ def _ptr(buf):
             raise ValueError("buffers must be CUDA tensors (device memory)")
         return buf.data_ptr()
     raise TypeError(f"unsupported buffer type {type(buf)}")
+
+
+def _host_ptr(buf):
+    """Address of a host buffer: a CPU torch tensor or a numpy array."""
+    if isinstance(buf, np.ndarray):
+        return buf.ctypes.data
+    if getattr(buf, "is_cuda", False):
+        raise ValueError("bine_allreduce_host takes host buffers")
+    return buf.data_ptr()
 
 
 def dtype_of_tensor(t):
@@ -248,6 +258,11 @@ class Comm:
     # ------------------------------------------------------ collectives
     def allreduce(self, sendbuf, recvbuf, count, datatype, op=SUM):
         check(lib().bine_allreduce(_ptr(sendbuf), _ptr(recvbuf), count, datatype, op, self._h))
+
+    def allreduce_host(self, sendbuf, recvbuf, count, datatype, op=SUM):
+        """bine_allreduce_host: host (CPU) tensors or numpy arrays, pinned
+        for full bandwidth; returns when recvbuf holds the result."""
+        check(lib().bine_allreduce_host(_host_ptr(sendbuf), _host_ptr(recvbuf), count, datatype, op, self._h))
 
     def reduce_scatter(self, sendbuf, recvbuf, recvcounts, datatype, op=SUM):
         rc = (ctypes.c_int * self.nranks)(*recvcounts)

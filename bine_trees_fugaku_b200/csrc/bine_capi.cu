@@ -91,7 +91,22 @@ struct DevTrees {
     dev::TreeTile* stiles = nullptr;
     int nstiles = 0;
     int smax_prog_len = 0;
+    // Host copies of the tile lists and segment offsets, for column windows.
+    std::vector<dev::TreeTile> h_tiles, h_stiles;
+    std::vector<int64_t> h_seg_off;
+    // Per window width: every window's clipped tiles (one-lane and split
+    // forms), with per-window begin indices.
+    struct Windows {
+        dev::TreeTile* tiles = nullptr;
+        dev::TreeTile* stiles = nullptr;
+        std::vector<int> begin, sbegin;
+    };
+    std::map<long long, Windows> windows;
     ~DevTrees() {
+        for (auto& kv : windows) {
+            cudaFree(kv.second.tiles);
+            cudaFree(kv.second.stiles);
+        }
         cudaFree(segs);
         cudaFree(prog);
         cudaFree(tiles);
@@ -162,10 +177,26 @@ struct bine_comm_s {
     int* status = nullptr;
     unsigned long long step_timeout_ns = 5ull * 1000 * 1000 * 1000;
     unsigned barrier_extra = 0;
+    // Host-buffer pipeline (bine_allreduce_host), created on first use:
+    // copy streams, per-slot events (input copied, reduced, output copied)
+    // and the device staging area (2 slots x input and output windows).
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_in[2] = {}, ev_reduced[2] = {}, ev_out[2] = {}, ev_start = nullptr;
+    char* stage = nullptr;
+    size_t stage_bytes = 0;
     ~bine_comm_s() {
         cudaFree(work);
         cudaFree(barrier);
         cudaFree(status);
+        cudaFree(stage);
+        for (int s = 0; s < 2; s++) {
+            if (ev_in[s]) cudaEventDestroy(ev_in[s]);
+            if (ev_reduced[s]) cudaEventDestroy(ev_reduced[s]);
+            if (ev_out[s]) cudaEventDestroy(ev_out[s]);
+        }
+        if (ev_start) cudaEventDestroy(ev_start);
+        if (h2d) cudaStreamDestroy(h2d);
+        if (d2h) cudaStreamDestroy(d2h);
     }
 };
 
@@ -384,6 +415,8 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
             tiles.push_back(dev::TreeTile{(int32_t)i, 0, st, std::min(tile, tp.segs[i].n - st)});
     d->ntiles = (int)tiles.size();
     d->vec_ok = vec;
+    d->h_tiles = tiles;
+    for (const OutSegment& sg : tp.segs) d->h_seg_off.push_back(sg.off);
     cudaError_t e1, e2, e3;
     fill(&d->segs, segs, &e1);
     fill(&d->prog, prog, &e2);
@@ -423,7 +456,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
                 d->smax_prog_len = std::max(d->smax_prog_len, e - b);
                 for (int j = 0; j <= K; j++) sparts.push_back(st.parts[i * (K + 1) + j] - b);
                 for (int j = 0; j < K; j++) scomb.push_back(dev::TreeComb{st.comb[i * K + j].first, st.comb[i * K + j].second});
-                const int64_t stile = (int64_t)(dev::kThreads / K) * (16 / es);
+                const int64_t stile = (int64_t)(dev::kThreads / K) * (16 / es);  // 8/K groups of 32 vectors
                 for (int64_t s0 = 0; s0 < sg.n; s0 += stile)
                     stiles.push_back(dev::TreeTile{(int32_t)i, 0, s0, std::min(stile, sg.n - s0)});
             }
@@ -438,6 +471,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
             if (f1 != cudaSuccess || f2 != cudaSuccess || f3 != cudaSuccess || f4 != cudaSuccess || f5 != cudaSuccess)
                 return fail(BINE_ERR_CUDA, "uploading the split reduction trees failed");
             d->nstiles = (int)stiles.size();
+            d->h_stiles = stiles;
             d->split_k = K;
         }
     }
@@ -516,7 +550,9 @@ int launch_sum_dt(bine_comm_t c, int dt, int mode, const char* in, long long ist
 }
 
 template <typename T, int K>
-int launch_tree_split(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost) {
+int launch_tree_split(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
+                      const dev::TreeTile* stiles, int nstiles) {
+    if (nstiles == 0) return BINE_SUCCESS;
     const size_t smem = (size_t)d.smax_prog_len * sizeof(dev::TreeEntry);
     auto kern = dev::k_tree_split<T, K>;
     if (smem > 200 * 1024) return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
@@ -526,30 +562,41 @@ int launch_tree_split(bine_comm_t c, const DevTrees& d, const char* in, long lon
     // One resident wave of blocks walking the tiles: consecutive tiles of a
     // block share a segment, so its program is staged once.
     const long long resident = (long long)std::max(1, per_sm) * std::max(1, c->num_sms);
-    const unsigned g = (unsigned)std::max(1LL, std::min<long long>(d.nstiles, resident));
-    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.ssegs, d.sprog, d.sparts, d.scomb, d.stiles,
-                                                d.nstiles);
+    const unsigned g = (unsigned)std::max(1LL, std::min<long long>(nstiles, resident));
+    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.ssegs, d.sprog, d.sparts, d.scomb, stiles,
+                                                nstiles);
     CUDA_TRY(cudaGetLastError());
     return BINE_SUCCESS;
 }
 
+// Evaluates the trees of `d` for all its tiles, or (windowed calls) for the
+// tiles given: `tiles`/`ntiles` of the one-lane form and `stiles`/`nstiles`
+// of the split form, clipped to one column window.
 template <typename T>
-int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost) {
-    if (d.ntiles == 0) return BINE_SUCCESS;
+int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
+                const dev::TreeTile* tiles = nullptr, int ntiles = -1, const dev::TreeTile* stiles = nullptr,
+                int nstiles = -1) {
+    if (!tiles) {
+        tiles = d.tiles;
+        ntiles = d.ntiles;
+        stiles = d.stiles;
+        nstiles = d.nstiles;
+    }
+    if (ntiles == 0) return BINE_SUCCESS;
     const size_t smem = (size_t)d.max_prog_len * sizeof(dev::TreeEntry);
     const bool vec = d.vec_ok && aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0;
     if (vec && d.split_k > 1) {
         switch (d.split_k) {
-        case 2: return launch_tree_split<T, 2>(c, d, in, ist, out, ost);
-        case 4: return launch_tree_split<T, 4>(c, d, in, ist, out, ost);
-        case 8: return launch_tree_split<T, 8>(c, d, in, ist, out, ost);
+        case 2: return launch_tree_split<T, 2>(c, d, in, ist, out, ost, stiles, nstiles);
+        case 4: return launch_tree_split<T, 4>(c, d, in, ist, out, ost, stiles, nstiles);
+        case 8: return launch_tree_split<T, 8>(c, d, in, ist, out, ost, stiles, nstiles);
         }
     }
     auto kern = vec ? dev::k_tree_vec<T> : dev::k_tree_scalar<T>;
     if (smem > 227 * 1024) return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
     if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    unsigned g = (unsigned)std::min<long long>(d.ntiles, (long long)std::max(1, c->num_sms) * 8);
-    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.segs, d.prog, d.tiles, d.ntiles);
+    unsigned g = (unsigned)std::min<long long>(ntiles, (long long)std::max(1, c->num_sms) * 8);
+    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.segs, d.prog, tiles, ntiles);
     CUDA_TRY(cudaGetLastError());
     return BINE_SUCCESS;
 }
@@ -700,6 +747,144 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
     case kGather: return launch_copy(c, dev::kCopyGather, in, ist, out, ost, count * es, root, es);
     }
     return fail(BINE_ERR_ARG, "unknown collective");
+}
+
+// ------------------------------------------------------ host-buffer path
+// Tiles of `d` clipped to each column window [i*W, min(count, (i+1)*W)),
+// uploaded once per window width.
+int window_tiles(bine_comm_t c, DevTrees& d, long long W, long long count, const DevTrees::Windows** out) {
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto it = d.windows.find(W);
+    if (it == d.windows.end()) {
+        auto clip = [&](const std::vector<dev::TreeTile>& in, long long c0, long long c1,
+                        std::vector<dev::TreeTile>* o) {
+            for (const dev::TreeTile& t : in) {
+                const long long lo = d.h_seg_off[t.seg] + t.start, hi = lo + t.n;
+                const long long a = std::max(lo, c0), b = std::min(hi, c1);
+                if (a < b) o->push_back(dev::TreeTile{t.seg, 0, a - d.h_seg_off[t.seg], b - a});
+            }
+        };
+        DevTrees::Windows w;
+        std::vector<dev::TreeTile> t, st;
+        for (long long c0 = 0; c0 < count; c0 += W) {
+            w.begin.push_back((int)t.size());
+            w.sbegin.push_back((int)st.size());
+            clip(d.h_tiles, c0, std::min(count, c0 + W), &t);
+            clip(d.h_stiles, c0, std::min(count, c0 + W), &st);
+        }
+        w.begin.push_back((int)t.size());
+        w.sbegin.push_back((int)st.size());
+        cudaError_t e1, e2;
+        fill(&w.tiles, t, &e1);
+        fill(&w.stiles, st, &e2);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            cudaFree(w.tiles);
+            cudaFree(w.stiles);
+            return fail(BINE_ERR_CUDA, "uploading window tiles failed");
+        }
+        it = d.windows.emplace(W, std::move(w)).first;
+    }
+    *out = &it->second;
+    return BINE_SUCCESS;
+}
+
+template <typename T>
+int launch_tree_window(bine_comm_t c, const DevTrees& d, const DevTrees::Windows* w, long long i, const char* in,
+                       long long ist, char* out, long long ost) {
+    if (!w) return launch_tree<T>(c, d, in, ist, out, ost);
+    return launch_tree<T>(c, d, in, ist, out, ost, w->tiles + w->begin[i], w->begin[i + 1] - w->begin[i],
+                          w->stiles + w->sbegin[i], w->sbegin[i + 1] - w->sbegin[i]);
+}
+
+// Allreduce of rank-major HOST arrays.  Column windows of the P rows flow
+// through two device slots on three streams: the host->device copy of
+// window i+1, the reduction of window i and the device->host copy of window
+// i-1 run at once, so both PCIe directions stay busy.  The fused kernels do
+// the reduction (exact trees with windowed tiles in the reference float
+// order), so results equal bine_allreduce's.
+int allreduce_host(bine_comm_t c, const void* sendbuf, void* recvbuf, long long count, int dt) {
+    const int es = dtype_size(dt);
+    if (es < 0) return fail(BINE_ERR_ARG, "invalid datatype");
+    if (count < 0) return fail(BINE_ERR_ARG, "negative count");
+    if (count > 0 && (!sendbuf || !recvbuf)) return fail(BINE_ERR_ARG, "null buffer");
+    const long long ist = c->send_stride ? (long long)c->send_stride : count * es;
+    const long long ost = c->recv_stride ? (long long)c->recv_stride : count * es;
+    if (ist < count * es || ost < count * es) return fail(BINE_ERR_ARG, "layout stride smaller than a rank row");
+    if (count == 0) return BINE_SUCCESS;
+    int rc = ensure_device(c);
+    if (rc) return rc;
+    if (!c->h2d) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming));
+        for (int s = 0; s < 2; s++) {
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in[s], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_reduced[s], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out[s], cudaEventDisableTiming));
+        }
+    }
+    const bool exact = (dt == BINE_FLOAT || dt == BINE_DOUBLE) && c->order == BINE_ORDER_REFERENCE;
+    std::shared_ptr<DevTrees> trees;
+    if (exact) {
+        rc = get_dev_trees(c, make_key(c, kAllreduce, count, 0), es, &trees);
+        if (rc) return rc;
+    }
+    // Windows of ~32 MiB over all ranks, 256-byte aligned; the element
+    // path of the exact trees (unaligned segments) takes one window.
+    const long long P = c->P;
+    long long W = ((32ll << 20) / (P * es)) / (256 / es) * (256 / es);
+    W = std::max<long long>(W, 256 / es);
+    if (W >= count || (exact && !trees->vec_ok)) W = count;
+    const long long pitch = (W * es + 255) / 256 * 256;
+    const size_t slot = (size_t)P * pitch;
+    if (c->stage_bytes < 4 * slot) {
+        CUDA_TRY(cudaDeviceSynchronize());
+        cudaFree(c->stage);
+        c->stage = nullptr;
+        c->stage_bytes = 0;
+        CUDA_TRY(cudaMalloc(&c->stage, 4 * slot));
+        c->stage_bytes = 4 * slot;
+    }
+    const DevTrees::Windows* win = nullptr;
+    if (exact && W < count) {
+        rc = window_tiles(c, *trees, W, count, &win);
+        if (rc) return rc;
+    }
+    // The pipeline starts after the work already queued on the
+    // communicator's stream and ends on it, so the call is stream-ordered.
+    CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
+    CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_start, 0));
+    const long long nwin = (count + W - 1) / W;
+    for (long long i = 0; i < nwin; i++) {
+        const int s = (int)(i & 1);
+        const long long c0 = i * W, w = std::min(W, count - c0);
+        char* in_s = c->stage + (size_t)(2 * s) * slot;
+        char* out_s = c->stage + (size_t)(2 * s + 1) * slot;
+        if (i >= 2) CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_reduced[s], 0));  // input slot consumed
+        CUDA_TRY(cudaMemcpy2DAsync(in_s, pitch, (const char*)sendbuf + c0 * es, ist, w * es, P,
+                                   cudaMemcpyHostToDevice, c->h2d));
+        CUDA_TRY(cudaEventRecord(c->ev_in[s], c->h2d));
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_in[s], 0));
+        if (i >= 2) CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_out[s], 0));  // output slot copied out
+        if (exact) {
+            // Element indices stay those of the full call: offset the bases.
+            const char* ib = in_s - c0 * es;
+            char* ob = out_s - c0 * es;
+            rc = dt == BINE_FLOAT ? launch_tree_window<float>(c, *trees, win, i, ib, pitch, ob, pitch)
+                                  : launch_tree_window<double>(c, *trees, win, i, ib, pitch, ob, pitch);
+        } else {
+            rc = launch_sum_dt(c, dt, dev::kSumAllreduce, in_s, pitch, out_s, pitch, w, 0, 0);
+        }
+        if (rc) return rc;
+        CUDA_TRY(cudaEventRecord(c->ev_reduced[s], c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(c->d2h, c->ev_reduced[s], 0));
+        CUDA_TRY(cudaMemcpy2DAsync((char*)recvbuf + c0 * es, ost, out_s, pitch, w * es, P, cudaMemcpyDeviceToHost,
+                                   c->d2h));
+        CUDA_TRY(cudaEventRecord(c->ev_out[s], c->d2h));
+    }
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_out[(nwin - 1) & 1], 0));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return BINE_SUCCESS;
 }
 
 int plan_for_query(bine_comm_t c, int coll, long count, int root, std::shared_ptr<Schedule>* s) {
@@ -1153,6 +1338,13 @@ int bine_allreduce(const void* sendbuf, void* recvbuf, int count, bine_datatype_
                    bine_comm_t comm) {
     if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
     return run_collective(comm, kAllreduce, sendbuf, recvbuf, count, datatype, 0);
+}
+
+int bine_allreduce_host(const void* sendbuf, void* recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
+                        bine_comm_t comm) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
+    return allreduce_host(comm, sendbuf, recvbuf, count, datatype);
 }
 
 int bine_reduce_scatter(const void* sendbuf, void* recvbuf, const int* recvcounts, bine_datatype_t datatype,

@@ -277,14 +277,16 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
     }
 }
 
-// Split form of k_tree_vec.  Each output vector is evaluated by a group of
-// K lanes of one warp: the host cut every segment's tree into K disjoint
-// subtrees (the "parts", in left-to-right order) and a combine program whose
-// leaves are the parts.  Lane j evaluates part j; the group exchanges the K
-// partial sums by shuffles and every lane runs the combine program, so the
-// additions and their association are exactly the tree's.  K times more,
-// K times shorter tasks remove the tail of the last wave when the output has
-// few vectors per resident thread.  Lanes then share the P output stores.
+// Split form of k_tree_vec.  The host cut every segment's addition tree
+// into K disjoint subtrees (the "parts", left to right) and a combine
+// program whose leaves are the parts.  A block of 8 warps owns 8/K column
+// groups of 32 vectors; warp w evaluates part w % K of group w / K, one
+// vector per lane, so every load of a warp is 512 contiguous bytes of one
+// rank row (as in k_sum_vec).  The partial sums meet in shared memory;
+// each warp then runs the combine program for its group's 32 vectors and
+// stores every K-th destination row.  The additions and their association
+// are exactly the tree's.  K times shorter tasks remove the tail of the
+// last wave when the output has few vectors per resident thread.
 struct TreeComb {  // combine entry: push part `part`, then `adds` additions
     int32_t part, adds;
 };
@@ -298,24 +300,28 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
                                                          const TreeComb* __restrict__ comb,
                                                          const TreeTile* __restrict__ tiles, int ntiles) {
     extern __shared__ TreeEntry sprog[];
+    constexpr int kWarps = kThreads / 32;
+    constexpr int kGroups = kWarps / K;
     __shared__ int spart[K + 1];
     __shared__ TreeComb scomb[K];
+    __shared__ uint4 partial[kWarps][32];
     constexpr int L = 16 / sizeof(T);
-    const int j = threadIdx.x % K;
-    const int gbase = (threadIdx.x & 31) & ~(K - 1);  // first lane of this group in the warp
+    constexpr int kRing = 4;  // loads in flight per lane (4 blocks of 256 threads fit per SM)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = warp % K, g = warp / K;
     int cur = -1;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const TreeTile tile = tiles[t];
         const TreeSeg sg = segs[tile.seg];
+        __syncthreads();  // the previous tile's partials and program are consumed
         if (tile.seg != cur) {  // block-uniform
-            __syncthreads();
             for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
             if (threadIdx.x <= K) spart[threadIdx.x] = parts[(long long)tile.seg * (K + 1) + threadIdx.x];
             if (threadIdx.x < K) scomb[threadIdx.x] = comb[(long long)tile.seg * K + threadIdx.x];
             __syncthreads();
             cur = tile.seg;
         }
-        const long long col = (long long)(threadIdx.x / K) * L;
+        const long long col = (long long)(g * 32 + lane) * L;
         const bool active = col < tile.n;
         const long long e = sg.off + tile.start + col;
         uint4 top = make_uint4(0, 0, 0, 0);
@@ -323,21 +329,21 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
             const int b = spart[j], len = spart[j + 1] - b;
             uint4 stk[kMaxTreeDepth];
             int sp = 0;
-            uint4 ring[4];
+            uint4 ring[kRing];
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < kRing; u++)
                 if (u < len) {
                     const TreeEntry q = sprog[b + u];
                     ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
                 }
-            for (int k0 = 0; k0 < len; k0 += 4) {
+            for (int k0 = 0; k0 < len; k0 += kRing) {
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
+                for (int u = 0; u < kRing; u++) {
                     const int k = k0 + u;
                     if (k < len) {
                         const uint4 v = ring[u];
-                        if (k + 4 < len) {
-                            const TreeEntry q = sprog[b + k + 4];
+                        if (k + kRing < len) {
+                            const TreeEntry q = sprog[b + k + kRing];
                             ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
                         }
                         if (k > 0) stk[sp++] = top;
@@ -347,25 +353,18 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
                 }
             }
         }
-        // Every lane of the warp takes part in the exchange (inactive lanes
-        // carry zeros nobody reads).
-        const uint4 mine = top;
+        partial[warp][lane] = top;
+        __syncthreads();
+        if (!active) continue;
         uint4 cstk[K];
         int csp = 0;
 #pragma unroll
         for (int q = 0; q < K; q++) {
             const TreeComb c = scomb[q];
-            const int src = gbase + c.part;
-            uint4 v;
-            v.x = __shfl_sync(0xffffffffu, mine.x, src);
-            v.y = __shfl_sync(0xffffffffu, mine.y, src);
-            v.z = __shfl_sync(0xffffffffu, mine.z, src);
-            v.w = __shfl_sync(0xffffffffu, mine.w, src);
             if (q > 0) cstk[csp++] = top;
-            top = v;
+            top = partial[g * K + c.part][lane];
             for (int a = c.adds; a > 0; a--) top = vadd<T>(cstk[--csp], top);
         }
-        if (!active) continue;
         if (sg.rank < 0) {
             for (int d = j; d < P; d += K) st_stream(out + (long long)d * out_stride + e * (long long)sizeof(T), top);
         } else if (j == 0) {

@@ -8,7 +8,9 @@ choices the reference leaves to LIBBINE_* variables and its sweep scripts.
 None of them changes a result: they only change time.
 
 * Features (one row per call): op one-hot, log2 P, log2 message bytes,
-  torus shape (number of dimensions and log2 of each), dtype one-hot.
+  torus shape (number of dimensions and log2 of each), dtype one-hot, and
+  derived terms (bytes per block, distance from a power of two, message
+  against the default segment).
 * Targets per arm: log2 measured GPU time and log2 of the busiest torus
   link's bytes, both generated by this engine (bench.py --suite picker).
 * Model: bine_mlp (3 x 256, GELU, bf16 weights, fp32 accumulation),
@@ -16,6 +18,8 @@ None of them changes a result: they only change time.
 * Judge: exhaustive search (every valid arm measured).  Fallback: the
   reference's fixed rule (fixed_rule below), used when no model is loaded
   or the model's pick is not valid for the call.
+* Picker.choose applies the model's best provable arm; Picker.tune times
+  the model's best few arms once per call shape and keeps the fastest.
 """
 import json
 import math
@@ -57,12 +61,16 @@ def message_bytes(coll, P, count, es):
     return count * es * P  # reduce_scatter send row / allgather receive row
 
 
+FEATURE_VERSION = 2
+
+
 def features(coll, P, count, es, dims=None):
     dims = list(dims or [P])
+    msg = max(1, message_bytes(coll, P, count, es))
     f = np.zeros(IN_DIM, np.float32)
     f[OPS.index(coll)] = 1.0
     f[3] = math.log2(P) / 12.0
-    f[4] = math.log2(max(1, message_bytes(coll, P, count, es))) / 28.0
+    f[4] = math.log2(msg) / 28.0
     f[5] = len(dims) / 3.0
     for i, d in enumerate(dims[:3]):
         f[6 + i] = math.log2(d) / 12.0
@@ -70,6 +78,10 @@ def features(coll, P, count, es, dims=None):
     f[10] = 1.0 if es != 4 else 0.0
     f[11] = 1.0 if is_p2(P) else 0.0
     f[12] = math.log2(max(1, count)) / 28.0
+    f[13] = math.log2(max(1.0, msg / P)) / 28.0  # bytes per block
+    lp = math.log2(P)
+    f[14] = lp - math.floor(lp)  # distance above the power of two below P
+    f[15] = min(1.0, msg / (32.0 * 1024))  # below/above the default 32 KiB segment
     return f
 
 
@@ -184,14 +196,37 @@ def sample_configs(n, seed, max_total_bytes=2 << 30):
     return out
 
 
+def time_arm(comm, coll, send, recv, count, code, stream, reps=3, target_us=300.0, max_batch=32):
+    """Microseconds per call: `reps` batches of back-to-back launches
+    between two CUDA events (the batch grows until it spans ~target_us),
+    median of the per-launch averages."""
+    import torch
+
+    def batch(n):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            comm.run(coll, send, recv, count, code)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e3 / n
+
+    first = batch(1)
+    n = int(min(max_batch, max(1, target_us // max(first, 1e-3))))
+    ts = [batch(n) for _ in range(reps)]
+    comm.synchronize()
+    return float(np.median(ts))
+
+
 def measure(configs, reps=3, time_budget_s=None, log=None):
     """Measures every valid arm of every call on the GPU with the STEPS
-    engine: median of `reps` launches timed with CUDA events, and the
-    busiest link's bytes from the engine's device link accounting.  Calls
+    engine (time_arm), and the busiest link's bytes from the engine's device link accounting.  Calls
     are grouped by torus so each communicator (and its proof cache) serves
     many calls.  Returns (configs measured, X [n, IN_DIM], T_us [n, NARMS],
-    L_bytes [n, NARMS], valid [n, NARMS]); arms the engine refuses are
-    invalid.  Stops early, keeping whole calls, once time_budget_s passes."""
+    L_bytes [n, NARMS], valid [n, NARMS]) in the order of `configs`; arms
+    the engine refuses are invalid.  Stops early, keeping whole calls, once
+    time_budget_s passes (the measured calls are then a subset)."""
     import time
 
     import torch
@@ -203,7 +238,7 @@ def measure(configs, reps=3, time_budget_s=None, log=None):
     perm = np.random.default_rng(0).permutation(len(keys))  # a budget stop keeps every P range
     group = {k: int(perm[j]) for j, k in enumerate(keys)}
     order = sorted(range(len(configs)), key=lambda i: (group[(configs[i]["P"], tuple(configs[i]["dims"]))], i))
-    cfgs, X, T, Lb = [], [], [], []
+    cfgs, X, T, Lb, done = [], [], [], [], []
     t_start = time.time()
     comm, comm_key = None, None
     for i in order:
@@ -235,21 +270,12 @@ def measure(configs, reps=3, time_budget_s=None, log=None):
                 comm.synchronize()
             except bine.BineError:
                 continue
-            ts = []
-            for _ in range(reps):
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                comm.run(coll, send, recv, count, code)
-                e1.record(stream)
-                e1.synchronize()
-                ts.append(e0.elapsed_time(e1) * 1e3)
-            comm.synchronize()
-            t_row[a] = float(np.median(ts))
+            t_row[a] = time_arm(comm, coll, send, recv, count, code, stream, reps)
             comm.link_bytes(coll, count, code, links)
             l_row[a] = float(links.max().item())
         del send, recv, links
         cfgs.append(cfg)
+        done.append(i)
         X.append(features(coll, P, count, es, dims))
         T.append(t_row)
         Lb.append(l_row)
@@ -257,19 +283,24 @@ def measure(configs, reps=3, time_budget_s=None, log=None):
             log(f"measured {len(cfgs)}/{len(configs)} calls in {time.time() - t_start:.0f} s (P={P})")
     if comm is not None:
         comm.close()
+    # Back to the callers' order (measurement ran grouped by torus).
+    back = sorted(range(len(cfgs)), key=lambda k: done[k])
+    cfgs = [cfgs[k] for k in back]
+    X, T, Lb = [X[k] for k in back], [T[k] for k in back], [Lb[k] for k in back]
     T = np.array(T).reshape(-1, NARMS)
     Lb = np.array(Lb).reshape(-1, NARMS)
     return cfgs, np.array(X, np.float32).reshape(-1, IN_DIM), T, Lb, ~np.isnan(T)
 
 
 # ------------------------------------------------------------- the model
-def targets(T, Lb, valid):
-    """Standardised log2 targets; returns (Y [n, OUT_DIM], mask, stats)."""
+def targets(T, Lb, valid, stats=None):
+    """Standardised log2 targets; returns (Y [n, OUT_DIM], mask, stats).
+    `stats` reuses another split's standardisation."""
     n = T.shape[0]
     lt = np.where(valid, np.log2(np.maximum(T, 1e-3)), 0.0)
     ll = np.where(valid, np.log2(np.maximum(Lb, 0.0) + 1.0), 0.0)
-    st = {"t_mean": float(lt[valid].mean()), "t_std": float(lt[valid].std() + 1e-9),
-          "l_mean": float(ll[valid].mean()), "l_std": float(ll[valid].std() + 1e-9)}
+    st = stats or {"t_mean": float(lt[valid].mean()), "t_std": float(lt[valid].std() + 1e-9),
+                   "l_mean": float(ll[valid].mean()), "l_std": float(ll[valid].std() + 1e-9)}
     Y = np.zeros((n, OUT_DIM), np.float32)
     M = np.zeros((n, OUT_DIM), np.float32)
     Y[:, :NARMS] = (lt - st["t_mean"]) / st["t_std"]
@@ -279,8 +310,10 @@ def targets(T, Lb, valid):
     return Y, M, st
 
 
-def train(X, Y, M, steps=3000, batch=256, lr=1e-3, seed=0, log=None):
-    """Trains bine_mlp on the GPU; returns (mlp, losses)."""
+def train(X, Y, M, steps=3000, batch=256, lr=1e-3, seed=0, log=None, val=None, check_every=250):
+    """Trains bine_mlp on the GPU (Adam, cosine learning rate); returns
+    (mlp, losses).  With val = (Xv, Yv, Mv) the parameters with the lowest
+    masked validation MSE seen at the checkpoints are kept."""
     import torch
 
     import bine_trees_fugaku_b200 as bine
@@ -290,13 +323,24 @@ def train(X, Y, M, steps=3000, batch=256, lr=1e-3, seed=0, log=None):
     n = X.shape[0]
     Xd, Yd, Md = (torch.from_numpy(a).cuda() for a in (X, Y, M))
     losses = []
+    best = (np.inf, None)
     for s in range(steps):
         idx = torch.from_numpy(rng.integers(0, n, batch)).cuda()
         cur = lr * 0.5 * (1 + math.cos(math.pi * s / steps))
         loss = mlp.train_step(Xd[idx].contiguous(), Yd[idx].contiguous(), Md[idx].contiguous(), cur)
         losses.append(loss)
-        if log and s % 500 == 0:
+        if val is not None and ((s + 1) % check_every == 0 or s + 1 == steps):
+            Xv, Yv, Mv = val
+            d = (predict(mlp, Xv) - Yv) * Mv
+            v = float((d * d).sum() / max(1.0, Mv.sum()))
+            if v < best[0]:
+                best = (v, mlp.get_params())
+            if log:
+                log(f"step {s + 1} train {loss:.4f} val {v:.4f}")
+        elif log and s % 500 == 0:
             log(f"step {s} loss {loss:.4f}")
+    if best[1] is not None:
+        mlp.set_params(best[1])
     return mlp, losses
 
 
@@ -314,15 +358,17 @@ def predict(mlp, X):
     return np.concatenate(out)[:n]
 
 
-def evaluate(pred, T, Lb, valid, configs):
+def evaluate(pred, T, Lb, valid, configs, shortlist=3):
     """Learned picks against exhaustive search (the measured optimum over
     every valid arm) and against the fixed rule, on held-out calls.
 
     Time objective: the arm with the lowest predicted time; its measured
-    time over the optimum's.  Link objective: the arm with the lowest
-    predicted busiest-link bytes; its bytes over the minimum."""
+    time over the optimum's.  Shortlist: the fastest measured of the
+    `shortlist` arms the model ranks best (what Picker.tune settles on).
+    Link objective: the arm with the lowest predicted busiest-link bytes;
+    its bytes over the minimum."""
     rows, within, ratio, speed, fixed_within, fixed_invalid = 0, 0, [], [], 0, 0
-    link_exact, link_ratio = 0, []
+    link_exact, link_ratio, short_within = 0, [], 0
     for i in range(T.shape[0]):
         v = valid[i]
         if not v.any():
@@ -332,6 +378,9 @@ def evaluate(pred, T, Lb, valid, configs):
         t_opt = float(np.min(T[i, v]))
         within += T[i, a] <= 1.05 * t_opt
         ratio.append(T[i, a] / t_opt)
+        # Shortlist: the best measured of the model's `shortlist` best arms.
+        top = np.argsort(np.where(v, pred[i, :NARMS], np.inf))[:min(shortlist, int(v.sum()))]
+        short_within += float(np.min(T[i, top])) <= 1.05 * t_opt
         c = configs[i]
         fa = fixed_rule(c["coll"], c["P"], c["count"], c["es"])
         if v[fa]:
@@ -348,6 +397,7 @@ def evaluate(pred, T, Lb, valid, configs):
             "pick_within_5pct_of_optimum": within / max(1, rows),
             "pick_time_over_optimum_geomean": gm(ratio),
             "pick_time_over_optimum_max": float(max(ratio)) if ratio else None,
+            f"shortlist{shortlist}_within_5pct_of_optimum": short_within / max(1, rows),
             "fixed_rule_within_5pct_of_optimum": fixed_within / max(1, rows - fixed_invalid),
             "speedup_vs_fixed_rule_geomean": gm(speed),
             "calls_where_fixed_rule_is_refused": fixed_invalid,
@@ -361,6 +411,7 @@ DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data
 def save(path, mlp, stats, meta):
     """Saves the weights as the bf16 values the forward pass uses (the
     master copies are fp32; forward rounds them to bf16)."""
+    meta = dict(meta, feature_version=FEATURE_VERSION)
     p = mlp.get_params()
     bits = (p.view(np.uint32) + 0x7FFF + ((p.view(np.uint32) >> 16) & 1)) >> 16  # round to nearest even
     np.savez_compressed(path, params_bf16=bits.astype(np.uint16), stats=json.dumps(stats),
@@ -389,9 +440,10 @@ class Picker:
         self.mlp = None
         self.cache = {}
         if path and os.path.exists(path):
-            p, dims, _, _, arms = load_params(path)
-            if [tuple(a) for a in arms] != ARMS or dims != (IN_DIM, 256, OUT_DIM):
-                raise ValueError(f"{path}: arm space or model shape differs from this build")
+            p, dims, _, meta, arms = load_params(path)
+            if [tuple(a) for a in arms] != ARMS or dims != (IN_DIM, 256, OUT_DIM) or \
+                    meta.get("feature_version") != FEATURE_VERSION:
+                raise ValueError(f"{path}: arm space, features or model shape differ from this build")
             self.mlp = bine.MLP(dims[0], dims[1], dims[2], 16, seed=0)
             self.mlp.set_params(p)
 
@@ -406,6 +458,45 @@ class Picker:
         x[0] = features(coll, P, count, es, dims)
         t = predict(self.mlp, x)[0, :NARMS]
         return sorted(ok, key=lambda a: t[a])
+
+    def tune(self, comm, coll, count, datatype, trials=3, reps=3):
+        """Times the `trials` best-ranked provable arms once for this call
+        shape on scratch buffers (the caller's data is not touched) and
+        caches the fastest; later choose() calls apply it.  Returns the arm."""
+        import torch
+
+        import bine_trees_fugaku_b200 as bine
+
+        es = bine.DTYPE_SIZE[datatype]
+        key = (coll, comm.nranks, tuple(comm.dims), count, es)
+        cands = []
+        for a in self.ranking(coll, comm.nranks, count, es, comm.dims):
+            apply_arm(comm, ARMS[a])
+            try:
+                comm.plan_verify(coll, count)
+            except bine.Unsupported:
+                continue
+            cands.append(a)
+            if len(cands) == trials:
+                break
+        if not cands:
+            raise bine.Unsupported(bine.ERR_UNSUPPORTED, f"no Bine schedule runs {coll} at P={comm.nranks}")
+        se, re = bine.row_counts(coll, count, comm.nranks)
+        tdt = {bine.INT32: torch.int32, bine.INT64: torch.int64, bine.FLOAT: torch.float32,
+               bine.DOUBLE: torch.float64, bine.CHAR: torch.int8}[datatype]
+        send = torch.zeros((comm.nranks, max(1, se)), dtype=tdt, device="cuda")
+        recv = torch.zeros((comm.nranks, re), dtype=tdt, device="cuda")
+        stream = torch.cuda.current_stream()
+        comm.set_stream(stream)
+        best = None
+        for a in cands:
+            apply_arm(comm, ARMS[a])
+            t = time_arm(comm, coll, send, recv, count, datatype, stream, reps)
+            if best is None or t < best[0]:
+                best = (t, a)
+        self.cache[key] = best[1]
+        apply_arm(comm, ARMS[best[1]])
+        return ARMS[best[1]]
 
     def choose(self, comm, coll, count, es):
         """Applies the best provable arm to `comm` and returns it."""

@@ -129,6 +129,19 @@ int bine_comm_set_float_order(bine_comm_t comm, int order);
 int bine_allreduce(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
                    bine_comm_t comm);
 
+/* MPI_Allreduce with HOST buffers, as an MPI caller holds them
+ * (lib/libbine.cc:1012): `sendbuf`/`recvbuf` are rank-major host arrays
+ * (strides from bine_comm_set_layout).  Column windows of ~32 MiB flow
+ * through the device on three streams so that the host->device copy of one
+ * window, the reduction of the previous one and the device->host copy of
+ * the one before that overlap.  Pinned host memory (cudaHostAlloc or
+ * cudaHostRegister) gives full PCIe bandwidth; pageable memory works at
+ * pageable-copy speed.  Returns when the result is in `recvbuf`.  Results
+ * equal bine_allreduce's (the fused kernels run whatever the engine
+ * setting; float sums follow the communicator's float order). */
+int bine_allreduce_host(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
+                        bine_comm_t comm);
+
 /* MPI_Reduce_scatter, lib/libbine.cc:1064 (recvcounts must all be equal, as
  * the reference's block implementation assumes, lib/libbine.cc:1065). */
 int bine_reduce_scatter(const void *sendbuf, void *recvbuf, const int *recvcounts, bine_datatype_t datatype,

@@ -366,3 +366,48 @@ def test_batched_launch_matches_semantics_and_single_calls():
                 ref = np.tile(full, (P, 1)) if coll == "allreduce" else full.reshape(P, c)
                 assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-30)
     b.close()
+
+
+@pytest.mark.parametrize("P,count,dt", [(256, (1 << 16) + 13, np.int32), (64, 300_000, np.int64), (7, 5, np.int8),
+                                        (512, 40_000, np.int32)])
+def test_allreduce_host_buffers_integers(P, count, dt):
+    """bine_allreduce_host on pinned host tensors: several column windows,
+    a ragged last window, exact integer sums (wrapping like C)."""
+    rng = np.random.default_rng(P + count)
+    x = rng.integers(-100, 101, (P, count)).astype(dt)
+    send = torch.from_numpy(x).pin_memory()
+    recv = torch.zeros_like(send).pin_memory()
+    comm = make_comm(P, "allreduce", "B")
+    comm.allreduce_host(send, recv, count, NP2CODE[x.dtype])
+    assert np.array_equal(recv.numpy(), expected("allreduce", x, P, count))
+
+
+@pytest.mark.parametrize("split", [0, 1, 8])
+def test_allreduce_host_buffers_float_reference_order(split):
+    """Exact-order float through column windows (P=256: 32,768 columns per
+    window) returns the device call's bits."""
+    P, count = 256, 256 * 200
+    x = np.random.default_rng(11).standard_normal((P, count)).astype(np.float32)
+    comm = make_comm(P, "allreduce", "B")
+    comm.set_tree_split(split)
+    dev = run(comm, "allreduce", x, count)
+    send = torch.from_numpy(x).pin_memory()
+    recv = torch.zeros_like(send).pin_memory()
+    comm.allreduce_host(send, recv, count, bine.FLOAT)
+    assert np.array_equal(recv.numpy().view(np.uint32), dev.view(np.uint32))
+
+
+def test_allreduce_host_pageable_in_place_and_strided():
+    P, count = 16, 5000
+    x = np.random.default_rng(3).integers(-1000, 1001, (P, count)).astype(np.int32)
+    comm = make_comm(P, "allreduce", "B")
+    buf = x.copy()  # pageable numpy memory, in place
+    comm.allreduce_host(buf, buf, count, bine.INT32)
+    assert np.array_equal(buf, expected("allreduce", x, P, count))
+    big = np.zeros((P, 6000), np.int32)
+    big[:, :count] = x
+    out = np.full((P, 6000), 7, np.int32)
+    comm.set_layout(6000 * 4, 6000 * 4)
+    comm.allreduce_host(big, out, count, bine.INT32)
+    assert np.array_equal(out[:, :count], expected("allreduce", x, P, count))
+    assert np.all(out[:, count:] == 7)

@@ -1,7 +1,7 @@
 """The learned picker against exhaustive search and the fixed rule, on the
-committed measurements (tests/golden/picker_dataset.npz: 1,500 sampled
+committed measurements (tests/golden/picker_dataset.npz: 3,000 sampled
 calls, every valid arm timed on a B200 with the STEPS engine, made by
-`python bench.py --suite picker`) and the committed weights trained on the
+`python bench.py --suite picker --picker-n 3000`) and the committed weights trained on the
 80 % of calls outside its `test` split.
 
 The CPU test evaluates the weights with the float64 reference of the MLP
@@ -19,6 +19,8 @@ from oracle import mlp_ref
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DATASET = os.path.join(HERE, "golden", "picker_dataset.npz")
+# The committed dataset: 3,000 sampled calls (bench.py --suite picker
+# --picker-n 3000), every valid arm timed on a B200 with the STEPS engine.
 
 
 def load():
@@ -37,13 +39,15 @@ def cpu_predict(X):
 def check_gain(ev):
     # Learned picks land within 5 % of the measured optimum on most
     # held-out calls, far more often than the fixed rule, and are faster
-    # than the fixed rule on average.
-    assert ev["held_out_calls"] >= 200
-    assert ev["pick_within_5pct_of_optimum"] >= 0.75
-    assert ev["pick_within_5pct_of_optimum"] >= ev["fixed_rule_within_5pct_of_optimum"] + 0.25
-    assert ev["pick_time_over_optimum_geomean"] <= 1.06
-    assert ev["speedup_vs_fixed_rule_geomean"] >= 1.12
-    assert ev["link_bytes_over_minimum_geomean"] <= 1.05
+    # than the fixed rule on average; the model's three best arms, timed,
+    # hold an arm within 5 % of the optimum on >= 95 % of the calls.
+    assert ev["held_out_calls"] >= 400
+    assert ev["pick_within_5pct_of_optimum"] >= 0.85
+    assert ev["pick_within_5pct_of_optimum"] >= ev["fixed_rule_within_5pct_of_optimum"] + 0.4
+    assert ev["pick_time_over_optimum_geomean"] <= 1.04
+    assert ev["shortlist3_within_5pct_of_optimum"] >= 0.95
+    assert ev["speedup_vs_fixed_rule_geomean"] >= 1.2
+    assert ev["link_bytes_over_minimum_geomean"] <= 1.02
 
 
 def test_dataset_is_consistent():
@@ -85,6 +89,23 @@ def test_learned_picks_on_the_gpu_match_the_cpu_reference():
     assert same >= 0.97 * int(valid[te].any(1).sum())
     ev = pk.evaluate(gpu, T[te], Lb[te], valid[te], [cfgs[i] for i in te])
     check_gain(ev)
+
+
+@pytest.mark.gpu
+def test_shortlist_tuning_keeps_the_fastest_of_three_and_the_call_is_correct():
+    import torch
+
+    picker = pk.Picker()
+    comm = bine.Comm(128)
+    comm.set_engine("steps")
+    arm = picker.tune(comm, "allreduce", 1 << 15, bine.INT32, trials=3)
+    assert picker.choose(comm, "allreduce", 1 << 15, 4) == arm
+    x = torch.randint(-1000, 1001, (128, 1 << 15), dtype=torch.int32, device="cuda")
+    y = torch.zeros_like(x)
+    comm.allreduce(x, y, 1 << 15, bine.INT32)
+    comm.synchronize()
+    assert torch.equal(y, x.sum(0, dtype=torch.int32).expand(128, 1 << 15))
+    comm.close()
 
 
 @pytest.mark.gpu
