@@ -150,7 +150,7 @@ def reference_time(steps, warmup, budget_s=150.0):
         return {"error": "reference run failed", "detail": j}
     t = j["median_s"]
     gbs = 2 * P_RANKS * count * ES / t / 1e9
-    sample = (f"P=256 allreduce, {count} int32 per rank ({'full workload' if count == COUNT else 'scaled sample'}), "
+    sample = (f"P={P_RANKS} allreduce, {count} int32 per rank ({'full workload' if count == COUNT else 'scaled sample'}), "
               f"{steps} timed calls after {warmup} warm-ups; per call: two barriers, wall time around one call, "
               f"max over ranks, median over calls (bench/bench.cc:289-318, 376-387)")
     return {"value": gbs, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference", "sample": sample,
@@ -233,6 +233,7 @@ def run_engine_arm(args):
     comm.set_engine(args.engine)
     comm.set_float_order(args.order)
     comm.set_tree_split(args.tree_split)
+    comm.set_host_window(args.host_window)
 
     def step():
         comm.allreduce(send, recv, COUNT, code)
@@ -867,6 +868,8 @@ def main():
     ap.add_argument("--dtype", default="int32", choices=["int32", "float"])
     ap.add_argument("--engine", default="fused", choices=["fused", "steps"])
     ap.add_argument("--order", default="reference", choices=["reference", "fast"])
+    ap.add_argument("--host-window", type=int, default=32 << 20,
+                    help="column-window bytes of the host-buffer pipeline (e2e leg)")
     ap.add_argument("--tree-split", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="lanes per output vector of the exact-order float kernel (0: chosen per call)")
     ap.add_argument("--suite", default="headline", choices=["headline", "batch", "picker", "sweep", "links"])

@@ -112,6 +112,7 @@ def lib():
         "bine_debug_set_barrier_extra": [vp, ctypes.c_uint],
         "bine_comm_set_tree_split": [vp, ctypes.c_int],
         "bine_allreduce_host": [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp],
+        "bine_comm_set_host_window": [vp, ctypes.c_longlong],
         "bine_comm_synchronize": [vp],
         "bine_allreduce": [vp, vp, i, i, i, vp],
         "bine_reduce_scatter": [vp, vp, ctypes.POINTER(ci), i, i, vp],
@@ -243,6 +244,10 @@ class Comm:
 
     def set_step_timeout(self, ms):
         check(lib().bine_comm_set_step_timeout(self._h, ms))
+
+    def set_host_window(self, window_bytes):
+        """Column-window bytes of allreduce_host's pipeline."""
+        check(lib().bine_comm_set_host_window(self._h, window_bytes))
 
     def set_tree_split(self, lanes):
         """Lanes per output vector of the exact-order float reduction

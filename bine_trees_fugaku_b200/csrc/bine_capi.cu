@@ -78,35 +78,44 @@ struct DevTrees {
     dev::TreeSeg* segs = nullptr;
     dev::TreeEntry* prog = nullptr;
     dev::TreeTile* tiles = nullptr;
-    int ntiles = 0;
+    int ntiles = 0;        // vector tiles (16-byte aligned bodies of segments)
+    dev::TreeTile* rtiles = nullptr;  // element tiles of the rest (unaligned programs, long pieces)
+    int nrtiles = 0;
+    dev::TreeTile* htiles = nullptr;  // short element pieces (heads and tails of vector bodies)
+    int nhtiles = 0;
+    dev::TreeTile* atiles = nullptr;  // element tiles of everything (unaligned layouts)
+    int natiles = 0;
     int max_prog_len = 0;
-    bool vec_ok = false;  // every offset and shift is a multiple of 16 bytes
+    int depth = 0;  // deepest evaluation stack of any program
     // Split form (k_tree_split), used when split_k > 1 and the layout is
     // 16-byte aligned: the same segments over the split programs.
     int split_k = 1;
+    int split_parts = 1;  // parts per tree: split_k or 2 * split_k
     dev::TreeSeg* ssegs = nullptr;
     dev::TreeEntry* sprog = nullptr;
     int* sparts = nullptr;
     dev::TreeComb* scomb = nullptr;
+    int* sassign = nullptr;  // per segment: 2K part indices by warp, then K + 1 offsets
     dev::TreeTile* stiles = nullptr;
     int nstiles = 0;
     int smax_prog_len = 0;
+    int sdepth = 0;  // deepest stack of any part or combine program
     // Host copies of the tile lists and segment offsets, for column windows.
-    std::vector<dev::TreeTile> h_tiles, h_stiles;
+    std::vector<dev::TreeTile> h_tiles, h_stiles, h_rtiles, h_htiles, h_atiles;
     std::vector<int64_t> h_seg_off;
-    // Per window width: every window's clipped tiles (one-lane and split
-    // forms), with per-window begin indices.
+    // Per window width: every window's clipped tiles of each list, with
+    // per-window begin indices (list k: tiles[k] + begin[k][i]).
     struct Windows {
-        dev::TreeTile* tiles = nullptr;
-        dev::TreeTile* stiles = nullptr;
-        std::vector<int> begin, sbegin;
+        dev::TreeTile* tiles[5] = {};
+        std::vector<int> begin[5];
     };
     std::map<long long, Windows> windows;
     ~DevTrees() {
-        for (auto& kv : windows) {
-            cudaFree(kv.second.tiles);
-            cudaFree(kv.second.stiles);
-        }
+        for (auto& kv : windows)
+            for (auto* t : kv.second.tiles) cudaFree(t);
+        cudaFree(rtiles);
+        cudaFree(htiles);
+        cudaFree(atiles);
         cudaFree(segs);
         cudaFree(prog);
         cudaFree(tiles);
@@ -114,6 +123,7 @@ struct DevTrees {
         cudaFree(sprog);
         cudaFree(sparts);
         cudaFree(scomb);
+        cudaFree(sassign);
         cudaFree(stiles);
     }
 };
@@ -167,6 +177,10 @@ struct bine_comm_s {
     std::unordered_map<StructKey, std::string, StructKeyHash> refuted_why;
     long long segment_bytes = 0;
     int64_t cached_moves = 0;  // moves held by `schedules`
+    // Side stream of the exact-order float kernels (element pieces run
+    // beside the vector tiles) and its fork / join events.
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int tree_split = 0;        // lanes per output vector in k_tree_split (0: chosen per call)
     // Device state, created on first use.
     int device = -1;
@@ -184,6 +198,7 @@ struct bine_comm_s {
     cudaEvent_t ev_in[2] = {}, ev_reduced[2] = {}, ev_out[2] = {}, ev_start = nullptr;
     char* stage = nullptr;
     size_t stage_bytes = 0;
+    long long host_window = 32ll << 20;  // bytes of one column window over all ranks
     ~bine_comm_s() {
         cudaFree(work);
         cudaFree(barrier);
@@ -195,6 +210,9 @@ struct bine_comm_s {
             if (ev_out[s]) cudaEventDestroy(ev_out[s]);
         }
         if (ev_start) cudaEventDestroy(ev_start);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (h2d) cudaStreamDestroy(h2d);
         if (d2h) cudaStreamDestroy(d2h);
     }
@@ -259,6 +277,9 @@ int ensure_device(bine_comm_t c) {
     CUDA_TRY(cudaMalloc(&c->status, sizeof(int)));
     CUDA_TRY(cudaMemset(c->barrier, 0, 2 * sizeof(unsigned)));
     CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     c->device = dev;
     return BINE_SUCCESS;
 }
@@ -398,79 +419,171 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
     auto d = std::make_shared<DevTrees>();
     std::vector<dev::TreeSeg> segs;
     std::vector<dev::TreeEntry> prog;
-    std::vector<dev::TreeTile> tiles;
-    bool vec = true;
-    for (const ProgEntry& e : tp.prog) {
-        prog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
-        if ((e.shift * es) % 16) vec = false;
-    }
+    for (const ProgEntry& e : tp.prog) prog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
     for (const OutSegment& sg : tp.segs) {
         segs.push_back(dev::TreeSeg{sg.off, sg.n, sg.rank, sg.prog_begin, sg.prog_len, sg.depth});
         d->max_prog_len = std::max(d->max_prog_len, sg.prog_len);
-        if ((sg.off * es) % 16 || (sg.n * es) % 16) vec = false;
     }
-    const int64_t tile = vec ? (int64_t)dev::kThreads * (16 / es) : (int64_t)dev::kThreads * 4;
-    for (size_t i = 0; i < tp.segs.size(); i++)
-        for (int64_t st = 0; st < tp.segs[i].n; st += tile)
-            tiles.push_back(dev::TreeTile{(int32_t)i, 0, st, std::min(tile, tp.segs[i].n - st)});
+    // Every segment whose program reads at 16-byte-aligned shifts gets a
+    // vector body: its elements from the first to the last 16-byte boundary
+    // of the output row.  Heads, tails and the other segments run through
+    // the element kernel (rtiles); atiles cover everything element-wise for
+    // layouts that are not 16-byte aligned.
+    const int64_t L = 16 / es;
+    std::vector<int64_t> body_lo(tp.segs.size(), 0), body_hi(tp.segs.size(), 0);
+    std::vector<dev::TreeTile> tiles, rtiles, htiles, atiles;
+    const int64_t vtile = (int64_t)dev::kThreads * L, etile = (int64_t)dev::kThreads * 4;
+    auto add_tiles = [](std::vector<dev::TreeTile>* v, int32_t seg, int64_t lo, int64_t hi, int64_t step) {
+        for (int64_t st = lo; st < hi; st += step) v->push_back(dev::TreeTile{seg, 0, st, std::min(step, hi - st)});
+    };
+    for (size_t i = 0; i < tp.segs.size(); i++) {
+        const OutSegment& sg = tp.segs[i];
+        bool pv = true;
+        for (int k = sg.prog_begin; k < sg.prog_begin + sg.prog_len; k++) pv &= (tp.prog[k].shift % L) == 0;
+        if (pv) {
+            const int64_t lo = (sg.off + L - 1) / L * L - sg.off, hi = (sg.off + sg.n) / L * L - sg.off;
+            if (lo < hi) {
+                body_lo[i] = lo;
+                body_hi[i] = hi;
+            }
+        }
+        add_tiles(&tiles, (int32_t)i, body_lo[i], body_hi[i], vtile);
+        // Element pieces shorter than one vector go to the staged kernel.
+        auto piece = [&](int64_t lo, int64_t hi) { add_tiles(hi - lo < L ? &htiles : &rtiles, (int32_t)i, lo, hi, etile); };
+        if (body_lo[i] < body_hi[i]) {
+            piece(0, body_lo[i]);
+            piece(body_hi[i], sg.n);
+        } else {
+            piece(0, sg.n);
+        }
+        add_tiles(&atiles, (int32_t)i, 0, sg.n, etile);
+    }
     d->ntiles = (int)tiles.size();
-    d->vec_ok = vec;
+    d->nrtiles = (int)rtiles.size();
+    d->nhtiles = (int)htiles.size();
+    d->natiles = (int)atiles.size();
+    // Stack slots the kernels index: measured on every program (values
+    // alive at once), not taken from the planner's labels.
+    d->depth = 1;
+    for (const OutSegment& sg : tp.segs) {
+        int sp = 0;
+        for (int i = sg.prog_begin; i < sg.prog_begin + sg.prog_len; i++) {
+            d->depth = std::max(d->depth, ++sp);
+            sp -= tp.prog[i].adds;
+            if (sp < 1) return fail(BINE_ERR_INTERNAL, "malformed reduction program");
+        }
+        if (sp != 1) return fail(BINE_ERR_INTERNAL, "malformed reduction program");
+    }
+    if (d->depth > dev::kMaxTreeDepth) return fail(BINE_ERR_UNSUPPORTED, "reduction tree deeper than supported");
     d->h_tiles = tiles;
+    d->h_rtiles = rtiles;
+    d->h_htiles = htiles;
+    d->h_atiles = atiles;
     for (const OutSegment& sg : tp.segs) d->h_seg_off.push_back(sg.off);
-    cudaError_t e1, e2, e3;
+    cudaError_t e1, e2, e3, e4, e5, e6;
     fill(&d->segs, segs, &e1);
     fill(&d->prog, prog, &e2);
     fill(&d->tiles, tiles, &e3);
-    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+    fill(&d->rtiles, rtiles, &e4);
+    fill(&d->htiles, htiles, &e5);
+    fill(&d->atiles, atiles, &e6);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess || e5 != cudaSuccess ||
+        e6 != cudaSuccess)
         return fail(BINE_ERR_CUDA, "uploading the reduction trees failed");
-    // Split form: K lanes per output vector when the output has too few
-    // vectors to fill the GPU several times over (the last wave of a
-    // one-vector-per-thread launch would run mostly empty).
-    if (vec) {
+    // Split form of the vector bodies: K lanes per output vector when the
+    // output has too few vectors to fill the GPU several times over.
+    if (!tiles.empty()) {
         int min_leaves = INT32_MAX;
-        long long vecs = 0;
-        for (const OutSegment& sg : tp.segs) {
-            min_leaves = std::min(min_leaves, sg.prog_len);  // one leaf per program entry
-            vecs += sg.n / (16 / es);
-        }
+        for (size_t i = 0; i < tp.segs.size(); i++)
+            if (body_lo[i] < body_hi[i]) min_leaves = std::min(min_leaves, tp.segs[i].prog_len);  // one leaf per entry
         int K = 1;
         if (c->tree_split > 0) {
             K = c->tree_split;
             while (K > 1 && min_leaves < K) K /= 2;
         } else {
-            const long long resident_threads = (long long)std::max(1, c->num_sms) * 2048;
-            while (K < 8 && vecs * K < 8 * resident_threads && min_leaves >= 16 * K * 2) K *= 2;
+            // Measured on B200: 4 lanes beat 1 and 8 from 2 to 64 MiB per
+            // rank (the one-lane form needs 74 registers, 3 blocks per SM;
+            // the split form 64, 4 blocks), so the automatic choice is 4
+            // wherever every part keeps at least 8 leaves.
+            while (K < 4 && min_leaves >= 16 * K) K *= 2;
         }
+        while (K > 1 && min_leaves < 2 * K) K /= 2;  // 2K parts of at least one leaf
         if (K > 1) {
-            SplitTrees st;
-            if (!split_trees(tp, K, &st, &err)) return fail(BINE_ERR_INTERNAL, err);
+            // K parts, one per warp, or 2K parts assigned longest first when
+            // that lowers the busiest warp's leaves by 5 % or more (trees of
+            // non-power-of-two P do not cut into K equal subtrees).
+            auto lpt = [&](const SplitTrees& t, int np, size_t seg, std::vector<std::vector<int>>* mine) {
+                const int32_t* po = &t.parts[seg * (np + 1)];
+                std::vector<int> order(np), load(K, 0);
+                mine->assign(K, {});
+                for (int j = 0; j < np; j++) order[j] = j;
+                std::stable_sort(order.begin(), order.end(),
+                                 [&](int x, int y) { return po[x + 1] - po[x] > po[y + 1] - po[y]; });
+                for (int p : order) {
+                    const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+                    (*mine)[w].push_back(p);
+                    load[w] += po[p + 1] - po[p];
+                }
+                return *std::max_element(load.begin(), load.end());
+            };
+            SplitTrees s1, s2;
+            if (!split_trees(tp, K, &s1, &err) || !split_trees(tp, 2 * K, &s2, &err)) return fail(BINE_ERR_INTERNAL, err);
+            long long max1 = 0, max2 = 0;
+            std::vector<std::vector<int>> tmp;
+            for (size_t i = 0; i < tp.segs.size(); i++) {
+                max1 += lpt(s1, K, i, &tmp);
+                max2 += lpt(s2, 2 * K, i, &tmp);
+            }
+            const bool two = max2 * 100 <= max1 * 95;
+            const SplitTrees& st = two ? s2 : s1;
+            const int KP = two ? 2 * K : K;
             if (st.max_depth > dev::kMaxTreeDepth) return fail(BINE_ERR_UNSUPPORTED, "reduction tree deeper than supported");
             std::vector<dev::TreeSeg> ssegs;
-            std::vector<int> sparts;
+            std::vector<int> sparts, sassign;
             std::vector<dev::TreeComb> scomb;
             std::vector<dev::TreeTile> stiles;
             for (size_t i = 0; i < tp.segs.size(); i++) {
                 const OutSegment& sg = tp.segs[i];
-                const int32_t b = st.parts[i * (K + 1)], e = st.parts[i * (K + 1) + K];
+                const int32_t* po = &st.parts[i * (KP + 1)];
+                const int32_t b = po[0], e = po[KP];
                 ssegs.push_back(dev::TreeSeg{sg.off, sg.n, sg.rank, b, e - b, sg.depth});
                 d->smax_prog_len = std::max(d->smax_prog_len, e - b);
-                for (int j = 0; j <= K; j++) sparts.push_back(st.parts[i * (K + 1) + j] - b);
-                for (int j = 0; j < K; j++) scomb.push_back(dev::TreeComb{st.comb[i * K + j].first, st.comb[i * K + j].second});
-                const int64_t stile = (int64_t)(dev::kThreads / K) * (16 / es);  // 8/K groups of 32 vectors
-                for (int64_t s0 = 0; s0 < sg.n; s0 += stile)
-                    stiles.push_back(dev::TreeTile{(int32_t)i, 0, s0, std::min(stile, sg.n - s0)});
+                for (int j = 0; j <= KP; j++) sparts.push_back(po[j] - b);
+                for (int j = 0; j < KP; j++) scomb.push_back(dev::TreeComb{st.comb[i * KP + j].first, st.comb[i * KP + j].second});
+                std::vector<std::vector<int>> mine;
+                lpt(st, KP, i, &mine);
+                std::vector<int> offs{0};
+                for (int w = 0; w < K; w++) {
+                    sassign.insert(sassign.end(), mine[w].begin(), mine[w].end());
+                    offs.push_back(offs.back() + (int)mine[w].size());
+                }
+                sassign.insert(sassign.end(), offs.begin(), offs.end());
+                add_tiles(&stiles, (int32_t)i, body_lo[i], body_hi[i], (int64_t)(dev::kThreads / K) * L);
             }
+            d->split_parts = KP;
             std::vector<dev::TreeEntry> sprog;
             for (const ProgEntry& e : st.prog) sprog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
-            cudaError_t f1, f2, f3, f4, f5;
+            cudaError_t f1, f2, f3, f4, f5, f6;
             fill(&d->ssegs, ssegs, &f1);
             fill(&d->sprog, sprog, &f2);
             fill(&d->sparts, sparts, &f3);
             fill(&d->scomb, scomb, &f4);
             fill(&d->stiles, stiles, &f5);
-            if (f1 != cudaSuccess || f2 != cudaSuccess || f3 != cudaSuccess || f4 != cudaSuccess || f5 != cudaSuccess)
+            fill(&d->sassign, sassign, &f6);
+            if (f1 != cudaSuccess || f2 != cudaSuccess || f3 != cudaSuccess || f4 != cudaSuccess || f5 != cudaSuccess ||
+                f6 != cudaSuccess)
                 return fail(BINE_ERR_CUDA, "uploading the split reduction trees failed");
             d->nstiles = (int)stiles.size();
+            // Stack slots: the deepest part program or combine program.
+            int cdepth = 1;
+            for (size_t q = 0; q < st.comb.size(); q += KP) {
+                int sp = 0;
+                for (int j = 0; j < KP; j++) {
+                    cdepth = std::max(cdepth, ++sp);
+                    sp -= st.comb[q + j].second;
+                }
+            }
+            d->sdepth = std::max(st.max_depth, cdepth);
             d->h_stiles = stiles;
             d->split_k = K;
         }
@@ -499,6 +612,25 @@ unsigned resident_blocks(bine_comm_t c, K kern, int threads, size_t smem) {
     return (unsigned)(per_sm * std::max(1, c->num_sms));
 }
 
+template <typename T, int COLS>
+int launch_sum_cols(bine_comm_t c, int mode, const char* in, long long ist, char* out, long long ost, int P,
+                    long long ncol, long long blk_vec, int root) {
+    const long long tiles = (ncol + COLS - 1) / COLS;
+    const unsigned g = (unsigned)std::min<long long>(
+        tiles, resident_blocks(c, dev::k_sum_vec<T, dev::kSumAllreduce, COLS>, dev::kThreads, 0));
+    if (mode == dev::kSumAllreduce)
+        dev::k_sum_vec<T, dev::kSumAllreduce, COLS><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol,
+                                                                                         blk_vec, root);
+    else if (mode == dev::kSumReduceScatter)
+        dev::k_sum_vec<T, dev::kSumReduceScatter, COLS><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P,
+                                                                                             ncol, blk_vec, root);
+    else
+        dev::k_sum_vec<T, dev::kSumReduce, COLS><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol,
+                                                                                      blk_vec, root);
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
 template <typename T>
 int launch_sum(bine_comm_t c, int mode, const char* in, long long ist, char* out, long long ost, long long elems,
                long long blk, int root) {
@@ -510,16 +642,18 @@ int launch_sum(bine_comm_t c, int mode, const char* in, long long ist, char* out
     if (vec) {
         const long long ncol = elems * es / 16;
         if (ncol > 0) {
-            const long long tiles = (ncol + dev::kSumCols - 1) / dev::kSumCols;
-            const unsigned g = (unsigned)std::min<long long>(
-                tiles, resident_blocks(c, dev::k_sum_vec<T, dev::kSumAllreduce>, dev::kThreads, 0));
             const long long blk_vec = mode == dev::kSumReduceScatter ? blk * es / 16 : 0;
-            if (mode == dev::kSumAllreduce)
-                dev::k_sum_vec<T, dev::kSumAllreduce><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol, blk_vec, root);
-            else if (mode == dev::kSumReduceScatter)
-                dev::k_sum_vec<T, dev::kSumReduceScatter><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol, blk_vec, root);
-            else
-                dev::k_sum_vec<T, dev::kSumReduce><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol, blk_vec, root);
+            // Row groups of at least 8 rows: 1 group up to P = 15, 2 up to
+            // 31, 4 up to 63, 8 beyond (tile widths 256 / 128 / 64 / 32).
+            const int cols = P < 16 ? 256 : (P < 32 ? 128 : (P < 64 ? 64 : 32));
+            int rc;
+            switch (cols) {
+            case 256: rc = launch_sum_cols<T, 256>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
+            case 128: rc = launch_sum_cols<T, 128>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
+            case 64: rc = launch_sum_cols<T, 64>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
+            default: rc = launch_sum_cols<T, 32>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
+            }
+            if (rc) return rc;
             done = ncol * 16 / es;
         }
     }
@@ -549,55 +683,127 @@ int launch_sum_dt(bine_comm_t c, int dt, int mode, const char* in, long long ist
     return fail(BINE_ERR_ARG, "bad datatype");
 }
 
-template <typename T, int K>
-int launch_tree_split(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
-                      const dev::TreeTile* stiles, int nstiles) {
-    if (nstiles == 0) return BINE_SUCCESS;
-    const size_t smem = (size_t)d.smax_prog_len * sizeof(dev::TreeEntry);
-    auto kern = dev::k_tree_split<T, K>;
-    if (smem > 200 * 1024) return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
-    if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+// Dynamic shared memory of the vector tree kernels: the segment's program
+// (16-byte entries), then, when it fits, the per-thread evaluation stacks
+// (`depth` slots of 16 bytes per thread).
+struct TreeSmem {
+    size_t bytes;
+    int stack_off;  // in 16-byte words
+    bool stack;
+};
+TreeSmem tree_smem(int prog_len, int depth) {
+    static_assert(sizeof(dev::TreeEntry) == 16, "program entries are 16-byte words");
+    const size_t prog = (size_t)std::max(1, prog_len) * 16;
+    const size_t stack = (size_t)std::max(1, depth) * dev::kThreads * 16;
+    const bool in_smem = stack <= 64 * 1024 && prog + stack <= 200 * 1024;
+    return TreeSmem{prog + (in_smem ? stack : 0), (int)(prog / 16), in_smem};
+}
+
+template <typename K>
+int launch_tree_kernel(bine_comm_t c, K kern, size_t smem, long long ntiles, unsigned* grid) {
+    // Static and dynamic shared memory together: above 48 KB the dynamic
+    // part needs the opt-in attribute, above 227 KB it cannot launch.
+    cudaFuncAttributes fa;
+    CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    if (smem + fa.sharedSizeBytes > 227 * 1024)
+        return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
+    if (smem + fa.sharedSizeBytes > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, dev::kThreads, smem));
     // One resident wave of blocks walking the tiles: consecutive tiles of a
     // block share a segment, so its program is staged once.
     const long long resident = (long long)std::max(1, per_sm) * std::max(1, c->num_sms);
-    const unsigned g = (unsigned)std::max(1LL, std::min<long long>(nstiles, resident));
-    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.ssegs, d.sprog, d.sparts, d.scomb, stiles,
-                                                nstiles);
+    *grid = (unsigned)std::max(1LL, std::min<long long>(ntiles, resident));
+    return BINE_SUCCESS;
+}
+
+template <typename T, int K>
+int launch_tree_split(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
+                      const dev::TreeTile* stiles, int nstiles) {
+    if (nstiles == 0) return BINE_SUCCESS;
+    const TreeSmem sm = tree_smem(d.smax_prog_len, d.sdepth);
+    auto kern = sm.stack ? dev::k_tree_split<T, K, true> : dev::k_tree_split<T, K, false>;
+    unsigned g = 0;
+    int rc = launch_tree_kernel(c, kern, sm.bytes, nstiles, &g);
+    if (rc) return rc;
+    kern<<<g, dev::kThreads, sm.bytes, c->stream>>>(in, ist, out, ost, c->P, d.ssegs, d.sprog, d.sparts, d.scomb,
+                                                    d.sassign, stiles, nstiles, d.split_parts, sm.stack_off);
     CUDA_TRY(cudaGetLastError());
     return BINE_SUCCESS;
 }
 
-// Evaluates the trees of `d` for all its tiles, or (windowed calls) for the
-// tiles given: `tiles`/`ntiles` of the one-lane form and `stiles`/`nstiles`
-// of the split form, clipped to one column window.
+// Tile lists of a launch: vector tiles (one-lane and split forms) and
+// element tiles (the remainder, or everything for unaligned layouts).
+struct TileSet {
+    // vector one-lane, vector split, element remainder, short element
+    // pieces, element all
+    const dev::TreeTile* t[5];
+    int n[5];
+};
+
+TileSet all_tiles(const DevTrees& d) {
+    return TileSet{{d.tiles, d.stiles, d.rtiles, d.htiles, d.atiles},
+                   {d.ntiles, d.nstiles, d.nrtiles, d.nhtiles, d.natiles}};
+}
+
+// Evaluates the trees of `d` over the tiles of `ts` (all of them, or one
+// column window's).  On a 16-byte-aligned layout the vector tiles (split
+// form when the plan has one) run on the communicator's stream while the
+// element pieces run beside them on a side stream (forked and joined by
+// events, which graph capture also records); otherwise every element tile
+// runs on the element kernel.
 template <typename T>
 int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
-                const dev::TreeTile* tiles = nullptr, int ntiles = -1, const dev::TreeTile* stiles = nullptr,
-                int nstiles = -1) {
-    if (!tiles) {
-        tiles = d.tiles;
-        ntiles = d.ntiles;
-        stiles = d.stiles;
-        nstiles = d.nstiles;
-    }
-    if (ntiles == 0) return BINE_SUCCESS;
-    const size_t smem = (size_t)d.max_prog_len * sizeof(dev::TreeEntry);
-    const bool vec = d.vec_ok && aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0;
-    if (vec && d.split_k > 1) {
-        switch (d.split_k) {
-        case 2: return launch_tree_split<T, 2>(c, d, in, ist, out, ost, stiles, nstiles);
-        case 4: return launch_tree_split<T, 4>(c, d, in, ist, out, ost, stiles, nstiles);
-        case 8: return launch_tree_split<T, 8>(c, d, in, ist, out, ost, stiles, nstiles);
+                const TileSet& ts) {
+    const bool vec = aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0;
+    unsigned g = 0;
+    int rc;
+    const bool side = vec && (ts.n[2] > 0 || ts.n[3] > 0);
+    cudaStream_t es = c->stream;
+    if (side) {
+        CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
+        CUDA_TRY(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+        es = c->side;
+        if (ts.n[3] > 0) {
+            const size_t prog = (size_t)std::max(1, d.max_prog_len) * sizeof(dev::TreeEntry);
+            const size_t smem = prog + (size_t)(16 / sizeof(T) - 1) * std::max(1, d.max_prog_len) * sizeof(T);
+            rc = launch_tree_kernel(c, dev::k_tree_staged<T>, smem, ts.n[3], &g);
+            if (rc) return rc;
+            dev::k_tree_staged<T><<<g, dev::kThreads, smem, es>>>(in, ist, out, ost, c->P, d.segs, d.prog, ts.t[3],
+                                                                  ts.n[3], (int)(prog / 16));
+            CUDA_TRY(cudaGetLastError());
         }
     }
-    auto kern = vec ? dev::k_tree_vec<T> : dev::k_tree_scalar<T>;
-    if (smem > 227 * 1024) return fail(BINE_ERR_UNSUPPORTED, "reduction program does not fit in shared memory");
-    if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    unsigned g = (unsigned)std::min<long long>(ntiles, (long long)std::max(1, c->num_sms) * 8);
-    kern<<<g, dev::kThreads, smem, c->stream>>>(in, ist, out, ost, c->P, d.segs, d.prog, tiles, ntiles);
-    CUDA_TRY(cudaGetLastError());
+    if (vec && d.split_k > 1 && ts.n[1] > 0) {
+        switch (d.split_k) {
+        case 2: rc = launch_tree_split<T, 2>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
+        case 4: rc = launch_tree_split<T, 4>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
+        default: rc = launch_tree_split<T, 8>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
+        }
+        if (rc) return rc;
+    } else if (vec && ts.n[0] > 0) {
+        const TreeSmem sm = tree_smem(d.max_prog_len, d.depth);
+        auto kern = sm.stack ? dev::k_tree_vec<T, true> : dev::k_tree_vec<T, false>;
+        rc = launch_tree_kernel(c, kern, sm.bytes, ts.n[0], &g);
+        if (rc) return rc;
+        kern<<<g, dev::kThreads, sm.bytes, c->stream>>>(in, ist, out, ost, c->P, d.segs, d.prog, ts.t[0], ts.n[0],
+                                                        sm.stack_off);
+        CUDA_TRY(cudaGetLastError());
+    }
+    const dev::TreeTile* et = vec ? ts.t[2] : ts.t[4];
+    const int ne = vec ? ts.n[2] : ts.n[4];
+    if (ne > 0) {
+        const size_t smem = (size_t)std::max(1, d.max_prog_len) * sizeof(dev::TreeEntry);
+        rc = launch_tree_kernel(c, dev::k_tree_scalar<T>, smem, ne, &g);
+        if (rc) return rc;
+        dev::k_tree_scalar<T><<<g, dev::kThreads, smem, es>>>(in, ist, out, ost, c->P, d.segs, d.prog, et, ne);
+        CUDA_TRY(cudaGetLastError());
+    }
+    if (side) {
+        CUDA_TRY(cudaEventRecord(c->ev_join, c->side));
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    }
     return BINE_SUCCESS;
 }
 
@@ -732,8 +938,8 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
             std::shared_ptr<DevTrees> d;
             rc = get_dev_trees(c, k, es, &d);
             if (rc) return rc;
-            return dt == BINE_FLOAT ? launch_tree<float>(c, *d, in, ist, out, ost)
-                                    : launch_tree<double>(c, *d, in, ist, out, ost);
+            return dt == BINE_FLOAT ? launch_tree<float>(c, *d, in, ist, out, ost, all_tiles(*d))
+                                    : launch_tree<double>(c, *d, in, ist, out, ost, all_tiles(*d));
         }
         const int mode = coll == kAllreduce ? dev::kSumAllreduce
                                             : (coll == kReduceScatter ? dev::kSumReduceScatter : dev::kSumReduce);
@@ -751,7 +957,8 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
 
 // ------------------------------------------------------ host-buffer path
 // Tiles of `d` clipped to each column window [i*W, min(count, (i+1)*W)),
-// uploaded once per window width.
+// uploaded once per window width.  W is a multiple of 16 bytes, so clipped
+// vector tiles stay aligned.
 int window_tiles(bine_comm_t c, DevTrees& d, long long W, long long count, const DevTrees::Windows** out) {
     std::lock_guard<std::mutex> lk(c->mu);
     auto it = d.windows.find(W);
@@ -764,23 +971,22 @@ int window_tiles(bine_comm_t c, DevTrees& d, long long W, long long count, const
                 if (a < b) o->push_back(dev::TreeTile{t.seg, 0, a - d.h_seg_off[t.seg], b - a});
             }
         };
+        const std::vector<dev::TreeTile>* lists[5] = {&d.h_tiles, &d.h_stiles, &d.h_rtiles, &d.h_htiles,
+                                                      &d.h_atiles};
         DevTrees::Windows w;
-        std::vector<dev::TreeTile> t, st;
-        for (long long c0 = 0; c0 < count; c0 += W) {
-            w.begin.push_back((int)t.size());
-            w.sbegin.push_back((int)st.size());
-            clip(d.h_tiles, c0, std::min(count, c0 + W), &t);
-            clip(d.h_stiles, c0, std::min(count, c0 + W), &st);
-        }
-        w.begin.push_back((int)t.size());
-        w.sbegin.push_back((int)st.size());
-        cudaError_t e1, e2;
-        fill(&w.tiles, t, &e1);
-        fill(&w.stiles, st, &e2);
-        if (e1 != cudaSuccess || e2 != cudaSuccess) {
-            cudaFree(w.tiles);
-            cudaFree(w.stiles);
-            return fail(BINE_ERR_CUDA, "uploading window tiles failed");
+        for (int k = 0; k < 5; k++) {
+            std::vector<dev::TreeTile> v;
+            for (long long c0 = 0; c0 < count; c0 += W) {
+                w.begin[k].push_back((int)v.size());
+                clip(*lists[k], c0, std::min(count, c0 + W), &v);
+            }
+            w.begin[k].push_back((int)v.size());
+            cudaError_t e;
+            fill(&w.tiles[k], v, &e);
+            if (e != cudaSuccess) {
+                for (auto* t : w.tiles) cudaFree(t);
+                return fail(BINE_ERR_CUDA, "uploading window tiles failed");
+            }
         }
         it = d.windows.emplace(W, std::move(w)).first;
     }
@@ -791,9 +997,13 @@ int window_tiles(bine_comm_t c, DevTrees& d, long long W, long long count, const
 template <typename T>
 int launch_tree_window(bine_comm_t c, const DevTrees& d, const DevTrees::Windows* w, long long i, const char* in,
                        long long ist, char* out, long long ost) {
-    if (!w) return launch_tree<T>(c, d, in, ist, out, ost);
-    return launch_tree<T>(c, d, in, ist, out, ost, w->tiles + w->begin[i], w->begin[i + 1] - w->begin[i],
-                          w->stiles + w->sbegin[i], w->sbegin[i + 1] - w->sbegin[i]);
+    if (!w) return launch_tree<T>(c, d, in, ist, out, ost, all_tiles(d));
+    TileSet ts;
+    for (int k = 0; k < 5; k++) {
+        ts.t[k] = w->tiles[k] + w->begin[k][i];
+        ts.n[k] = w->begin[k][i + 1] - w->begin[k][i];
+    }
+    return launch_tree<T>(c, d, in, ist, out, ost, ts);
 }
 
 // Allreduce of rank-major HOST arrays.  Column windows of the P rows flow
@@ -829,12 +1039,16 @@ int allreduce_host(bine_comm_t c, const void* sendbuf, void* recvbuf, long long 
         rc = get_dev_trees(c, make_key(c, kAllreduce, count, 0), es, &trees);
         if (rc) return rc;
     }
-    // Windows of ~32 MiB over all ranks, 256-byte aligned; the element
-    // path of the exact trees (unaligned segments) takes one window.
+    // Windows of at most host_window bytes over all ranks (default 32 MiB),
+    // 256-byte aligned.
     const long long P = c->P;
-    long long W = ((32ll << 20) / (P * es)) / (256 / es) * (256 / es);
+    // At least ~8 windows once a call moves more than 16 MiB, so that the
+    // copies in and out overlap even for calls below one full window.
+    const long long total = P * count * es;
+    const long long wbytes = std::min<long long>(c->host_window, std::max<long long>(2ll << 20, total / 8));
+    long long W = (wbytes / (P * es)) / (256 / es) * (256 / es);
     W = std::max<long long>(W, 256 / es);
-    if (W >= count || (exact && !trees->vec_ok)) W = count;
+    if (W >= count) W = count;
     const long long pitch = (W * es + 255) / 256 * 256;
     const size_t slot = (size_t)P * pitch;
     if (c->stage_bytes < 4 * slot) {
@@ -1405,6 +1619,13 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms) {
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     comm->barrier_extra = extra;
+    return BINE_SUCCESS;
+}
+
+int bine_comm_set_host_window(bine_comm_t comm, long long window_bytes) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (window_bytes < 4096) return fail(BINE_ERR_ARG, "host window below 4 KiB");
+    comm->host_window = window_bytes;
     return BINE_SUCCESS;
 }
 

@@ -116,30 +116,32 @@ __device__ __forceinline__ uint4 vadd(uint4 a, uint4 b) {
 // ------------------------------------------------------- fused reductions
 enum SumMode { kSumAllreduce = 0, kSumReduceScatter = 1, kSumReduce = 2 };
 
-// Column sums over 16-byte vector columns.  A block owns tiles of
-// kSumCols vector columns at a time; its 8 warps split the P rows of a
-// tile (warp g sums rows [g*P/8, (g+1)*P/8) of its lane's column, 8 loads in
-// flight per thread), the partial sums meet in shared memory, and all 256
-// threads then store the result rows.  Tiles are small (kSumCols * P * 16
-// bytes of input) and handed out grid-stride, so the load balances across
-// the 148 SMs with no wave tail.  `ncol` vector columns per input row;
+// Column sums over 16-byte vector columns.  A block owns tiles of COLS
+// vector columns at a time; its 256 threads form 256/COLS row groups that
+// split the P rows of a tile (group g sums rows [g*P/G, (g+1)*P/G) of its
+// lane's column, 8 loads in flight per thread), the partial sums meet in
+// shared memory, and all threads then store the result rows.  The host
+// picks COLS from P so that every group has at least 8 rows (wide tiles
+// for small P, 32 columns and 8 groups from P = 64).  Tiles are handed out
+// grid-stride over the resident blocks, so the load balances across the
+// 148 SMs with no wave tail.  `ncol` vector columns per input row;
 // reduce_scatter: `blk` vector columns per destination rank.
-constexpr int kSumCols = 32;
-constexpr int kSumGroups = kThreads / kSumCols;
+constexpr int kSumCols = 32;  // the narrowest tile
 
-template <typename T, int MODE>
+template <typename T, int MODE, int COLS>
 __global__ void __launch_bounds__(kThreads) k_sum_vec(const char* __restrict__ in, long long in_stride,
                                                       char* __restrict__ out, long long out_stride, int P,
                                                       long long ncol, long long blk, int root) {
     using A = typename AccOf<T>::type;
-    __shared__ Lanes<T, A> part[kSumGroups][kSumCols];
-    __shared__ uint4 res[kSumCols];
-    const int lane = threadIdx.x % kSumCols, grp = threadIdx.x / kSumCols;
-    const int per = (P + kSumGroups - 1) / kSumGroups;
+    constexpr int G = kThreads / COLS;
+    __shared__ Lanes<T, A> part[G][COLS];
+    __shared__ uint4 res[COLS];
+    const int lane = threadIdx.x % COLS, grp = threadIdx.x / COLS;
+    const int per = (P + G - 1) / G;
     const int r0 = min(P, grp * per), r1 = min(P, r0 + per);
-    const long long ntiles = (ncol + kSumCols - 1) / kSumCols;
+    const long long ntiles = (ncol + COLS - 1) / COLS;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long col = tile * kSumCols + lane;
+        const long long col = tile * COLS + lane;
         Lanes<T, A> acc;
         acc.zero();
         if (col < ncol) {
@@ -154,22 +156,26 @@ __global__ void __launch_bounds__(kThreads) k_sum_vec(const char* __restrict__ i
             }
             for (; r < r1; r++) acc.add(ld_stream(p + (long long)r * in_stride));
         }
-        part[grp][lane] = acc;
-        __syncthreads();
-        if (grp == 0) {
-            Lanes<T, A> s = part[0][lane];
+        if (G > 1) {
+            part[grp][lane] = acc;
+            __syncthreads();
+            if (grp == 0) {
+                Lanes<T, A> sum = part[0][lane];
 #pragma unroll
-            for (int g = 1; g < kSumGroups; g++)
+                for (int g = 1; g < G; g++)
 #pragma unroll
-                for (int i = 0; i < Lanes<T, A>::N; i++) s.v[i] = add_exact<A>(s.v[i], part[g][lane].v[i]);
-            res[lane] = s.pack();
+                    for (int i = 0; i < Lanes<T, A>::N; i++) sum.v[i] = add_exact<A>(sum.v[i], part[g][lane].v[i]);
+                res[lane] = sum.pack();
+            }
+            __syncthreads();
+        } else {
+            res[lane] = acc.pack();
         }
-        __syncthreads();
         if (col < ncol) {
             const uint4 v = res[lane];
             if (MODE == kSumAllreduce) {
                 char* q = out + col * 16;
-                for (int d = grp; d < P; d += kSumGroups) st_stream(q + (long long)d * out_stride, v);
+                for (int d = grp; d < P; d += G) st_stream(q + (long long)d * out_stride, v);
             } else if (grp == 0) {
                 if (MODE == kSumReduceScatter) {
                     const long long owner = col / blk;
@@ -179,7 +185,7 @@ __global__ void __launch_bounds__(kThreads) k_sum_vec(const char* __restrict__ i
                 }
             }
         }
-        __syncthreads();
+        if (G > 1) __syncthreads();
     }
 }
 
@@ -222,15 +228,42 @@ struct TreeTile {  // `n` elements starting `start` elements into segment `seg`
     int64_t start, n;
 };
 
+// Evaluation stack of a postfix program (the entries below the top, which
+// stays in registers).  SMEM: in the block's dynamic shared memory, slot j
+// of thread t at base[j * kThreads + t], so a warp's 16-byte accesses fall
+// on consecutive words; sized by the host to the programs' Sethi-Ullman
+// depth.  Otherwise a local array (deep programs only): its indexing is
+// dynamic, so it lives in local memory and its traffic reaches L2.
+template <bool SMEM>
+struct EvalStack;
+template <>
+struct EvalStack<true> {
+    uint4* base;
+    __device__ __forceinline__ void init(uint4* smem_stack) { base = smem_stack + threadIdx.x; }
+    __device__ __forceinline__ void set(int j, uint4 v) { base[j * kThreads] = v; }
+    __device__ __forceinline__ uint4 get(int j) const { return base[j * kThreads]; }
+};
+template <>
+struct EvalStack<false> {
+    uint4 a[kMaxTreeDepth];
+    __device__ __forceinline__ void init(uint4*) {}
+    __device__ __forceinline__ void set(int j, uint4 v) { a[j] = v; }
+    __device__ __forceinline__ uint4 get(int j) const { return a[j]; }
+};
+
 // Vector form: every shift and offset is a multiple of 16 bytes.  One tile
 // per block; each thread owns one 16-byte column of the tile.
-template <typename T>
+template <typename T, bool SMEM>
 __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ in, long long in_stride,
                                                        char* __restrict__ out, long long out_stride, int P,
                                                        const TreeSeg* __restrict__ segs,
                                                        const TreeEntry* __restrict__ prog,
-                                                       const TreeTile* __restrict__ tiles, int ntiles) {
-    extern __shared__ TreeEntry sprog[];
+                                                       const TreeTile* __restrict__ tiles, int ntiles,
+                                                       int stack_off) {
+    extern __shared__ uint4 sdyn[];
+    TreeEntry* sprog = reinterpret_cast<TreeEntry*>(sdyn);
+    EvalStack<SMEM> stk;
+    stk.init(sdyn + stack_off);
     constexpr int L = 16 / sizeof(T);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const TreeTile tile = tiles[t];
@@ -241,7 +274,6 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
         const long long col = (long long)threadIdx.x * L;
         if (col >= tile.n) continue;
         const long long e = sg.off + tile.start + col;  // output element
-        uint4 stk[kMaxTreeDepth];
         uint4 top = make_uint4(0, 0, 0, 0);
         int sp = 0;
         const int len = sg.prog_len;
@@ -263,9 +295,9 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
                         const TreeEntry q = sprog[k + 8];
                         ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
                     }
-                    if (k > 0) stk[sp++] = top;
+                    if (k > 0) stk.set(sp++, top);
                     top = v;
-                    for (int a = sprog[k].adds; a > 0; a--) top = vadd<T>(stk[--sp], top);
+                    for (int a = sprog[k].adds; a > 0; a--) top = vadd<T>(stk.get(--sp), top);
                 }
             }
         }
@@ -278,35 +310,79 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
 }
 
 // Split form of k_tree_vec.  The host cut every segment's addition tree
-// into K disjoint subtrees (the "parts", left to right) and a combine
-// program whose leaves are the parts.  A block of 8 warps owns 8/K column
-// groups of 32 vectors; warp w evaluates part w % K of group w / K, one
-// vector per lane, so every load of a warp is 512 contiguous bytes of one
-// rank row (as in k_sum_vec).  The partial sums meet in shared memory;
+// into `nparts` disjoint subtrees (the "parts", left to right; K of them,
+// or 2K when that balances the warps better) and a combine program whose
+// leaves are the parts, and assigned the parts to K warps longest first, so
+// the warps carry near-equal numbers of leaves even when the tree is
+// unbalanced (non-power-of-two P).  A block of 8 warps owns 8/K
+// column groups of 32 vectors; warp w evaluates its parts for group w / K,
+// one vector per lane, so every load of a warp is 512 contiguous bytes of
+// one rank row (as in k_sum_vec).  The partial sums meet in shared memory;
 // each warp then runs the combine program for its group's 32 vectors and
 // stores every K-th destination row.  The additions and their association
-// are exactly the tree's.  K times shorter tasks remove the tail of the
-// last wave when the output has few vectors per resident thread.
+// are exactly the tree's.  Shorter tasks remove the tail of the last wave
+// when the output has few vectors per resident thread.
 struct TreeComb {  // combine entry: push part `part`, then `adds` additions
     int32_t part, adds;
 };
 
-template <typename T, int K>
+// Evaluates program entries [b, b + len) for element `e` (one 16-byte
+// vector), loads kRing entries ahead of the additions.
+template <typename T, bool SMEM, int kRing>
+__device__ __forceinline__ uint4 eval_program(const char* __restrict__ in, long long in_stride, long long e,
+                                              const TreeEntry* sprog, int b, int len, EvalStack<SMEM>& stk) {
+    uint4 top = make_uint4(0, 0, 0, 0);
+    int sp = 0;
+    uint4 ring[kRing];
+#pragma unroll
+    for (int u = 0; u < kRing; u++)
+        if (u < len) {
+            const TreeEntry q = sprog[b + u];
+            ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+        }
+    for (int k0 = 0; k0 < len; k0 += kRing) {
+#pragma unroll
+        for (int u = 0; u < kRing; u++) {
+            const int k = k0 + u;
+            if (k < len) {
+                const uint4 v = ring[u];
+                if (k + kRing < len) {
+                    const TreeEntry q = sprog[b + k + kRing];
+                    ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                }
+                if (k > 0) stk.set(sp++, top);
+                top = v;
+                for (int a = sprog[b + k].adds; a > 0; a--) top = vadd<T>(stk.get(--sp), top);
+            }
+        }
+    }
+    return top;
+}
+
+template <typename T, int K, bool SMEM>
 __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict__ in, long long in_stride,
                                                          char* __restrict__ out, long long out_stride, int P,
                                                          const TreeSeg* __restrict__ segs,
                                                          const TreeEntry* __restrict__ prog,
                                                          const int* __restrict__ parts,
                                                          const TreeComb* __restrict__ comb,
-                                                         const TreeTile* __restrict__ tiles, int ntiles) {
-    extern __shared__ TreeEntry sprog[];
+                                                         const int* __restrict__ assign,
+                                                         const TreeTile* __restrict__ tiles, int ntiles,
+                                                         int nparts, int stack_off) {
+    extern __shared__ uint4 sdyn[];
+    TreeEntry* sprog = reinterpret_cast<TreeEntry*>(sdyn);
+    EvalStack<SMEM> stk;
+    stk.init(sdyn + stack_off);
     constexpr int kWarps = kThreads / 32;
     constexpr int kGroups = kWarps / K;
-    __shared__ int spart[K + 1];
-    __shared__ TreeComb scomb[K];
-    __shared__ uint4 partial[kWarps][32];
+    constexpr int KP = 2 * K;
+    // Per segment: part offsets, combine program, and the parts of each warp
+    // (nparts <= KP part indices ordered by warp, then K + 1 offsets).
+    __shared__ int spart[KP + 1];
+    __shared__ TreeComb scomb[KP];
+    __shared__ int sasg[KP + K + 1];
+    __shared__ uint4 partial[kGroups][KP][32];
     constexpr int L = 16 / sizeof(T);
-    constexpr int kRing = 4;  // loads in flight per lane (4 blocks of 256 threads fit per SM)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = warp % K, g = warp / K;
     int cur = -1;
@@ -316,59 +392,87 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
         __syncthreads();  // the previous tile's partials and program are consumed
         if (tile.seg != cur) {  // block-uniform
             for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
-            if (threadIdx.x <= K) spart[threadIdx.x] = parts[(long long)tile.seg * (K + 1) + threadIdx.x];
-            if (threadIdx.x < K) scomb[threadIdx.x] = comb[(long long)tile.seg * K + threadIdx.x];
+            if (threadIdx.x <= nparts) spart[threadIdx.x] = parts[(long long)tile.seg * (nparts + 1) + threadIdx.x];
+            if (threadIdx.x < nparts) scomb[threadIdx.x] = comb[(long long)tile.seg * nparts + threadIdx.x];
+            if (threadIdx.x < nparts + K + 1)
+                sasg[threadIdx.x] = assign[(long long)tile.seg * (nparts + K + 1) + threadIdx.x];
             __syncthreads();
             cur = tile.seg;
         }
         const long long col = (long long)(g * 32 + lane) * L;
         const bool active = col < tile.n;
         const long long e = sg.off + tile.start + col;
-        uint4 top = make_uint4(0, 0, 0, 0);
         if (active) {
-            const int b = spart[j], len = spart[j + 1] - b;
-            uint4 stk[kMaxTreeDepth];
-            int sp = 0;
-            uint4 ring[kRing];
-#pragma unroll
-            for (int u = 0; u < kRing; u++)
-                if (u < len) {
-                    const TreeEntry q = sprog[b + u];
-                    ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
-                }
-            for (int k0 = 0; k0 < len; k0 += kRing) {
-#pragma unroll
-                for (int u = 0; u < kRing; u++) {
-                    const int k = k0 + u;
-                    if (k < len) {
-                        const uint4 v = ring[u];
-                        if (k + kRing < len) {
-                            const TreeEntry q = sprog[b + k + kRing];
-                            ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
-                        }
-                        if (k > 0) stk[sp++] = top;
-                        top = v;
-                        for (int a = sprog[b + k].adds; a > 0; a--) top = vadd<T>(stk[--sp], top);
-                    }
-                }
+            for (int pi = sasg[nparts + j]; pi < sasg[nparts + j + 1]; pi++) {
+                const int p = sasg[pi];
+                partial[g][p][lane] =
+                    eval_program<T, SMEM, 4>(in, in_stride, e, sprog, spart[p], spart[p + 1] - spart[p], stk);
             }
         }
-        partial[warp][lane] = top;
         __syncthreads();
         if (!active) continue;
-        uint4 cstk[K];
-        int csp = 0;
-#pragma unroll
-        for (int q = 0; q < K; q++) {
+        uint4 top = make_uint4(0, 0, 0, 0);
+        int csp = 0;  // the parts' stack is empty again: the combine reuses it
+        for (int q = 0; q < nparts; q++) {
             const TreeComb c = scomb[q];
-            if (q > 0) cstk[csp++] = top;
-            top = partial[g * K + c.part][lane];
-            for (int a = c.adds; a > 0; a--) top = vadd<T>(cstk[--csp], top);
+            if (q > 0) stk.set(csp++, top);
+            top = partial[g][c.part][lane];
+            for (int a = c.adds; a > 0; a--) top = vadd<T>(stk.get(--csp), top);
         }
         if (sg.rank < 0) {
             for (int d = j; d < P; d += K) st_stream(out + (long long)d * out_stride + e * (long long)sizeof(T), top);
         } else if (j == 0) {
             st_stream(out + (long long)sg.rank * out_stride + e * (long long)sizeof(T), top);
+        }
+    }
+}
+
+// Element form for the short head and tail pieces of segments (fewer
+// elements than one 16-byte vector): the block first loads every leaf value
+// of the tile's elements into shared memory in one parallel round, then
+// one thread per element evaluates the program from there.  The leaf loads
+// of a program are thus issued together instead of one after another.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_tree_staged(const char* __restrict__ in, long long in_stride,
+                                                          char* __restrict__ out, long long out_stride, int P,
+                                                          const TreeSeg* __restrict__ segs,
+                                                          const TreeEntry* __restrict__ prog,
+                                                          const TreeTile* __restrict__ tiles, int ntiles,
+                                                          int vals_off) {
+    extern __shared__ uint4 sdyn[];
+    TreeEntry* sprog = reinterpret_cast<TreeEntry*>(sdyn);
+    T* vals = reinterpret_cast<T*>(sdyn + vals_off);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const TreeTile tile = tiles[t];
+        const TreeSeg sg = segs[tile.seg];
+        const int len = sg.prog_len;
+        __syncthreads();
+        for (int i = threadIdx.x; i < len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
+        __syncthreads();
+        const int total = (int)tile.n * len;
+        for (int i = threadIdx.x; i < total; i += blockDim.x) {
+            const int j = i / len, k = i - j * len;
+            const TreeEntry q = sprog[k];
+            const long long e = sg.off + tile.start + j;
+            vals[i] = *(const T*)(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+        }
+        __syncthreads();
+        if (threadIdx.x < tile.n) {
+            const int j = threadIdx.x;
+            const long long e = sg.off + tile.start + j;
+            T stk[kMaxTreeDepth];
+            T top = (T)0;
+            int sp = 0;
+            for (int k = 0; k < len; k++) {
+                if (k > 0) stk[sp++] = top;
+                top = vals[j * len + k];
+                for (int a = sprog[k].adds; a > 0; a--) top = add_exact<T>(stk[--sp], top);
+            }
+            if (sg.rank < 0) {
+                for (int d = 0; d < P; d++) *(T*)(out + (long long)d * out_stride + e * (long long)sizeof(T)) = top;
+            } else {
+                *(T*)(out + (long long)sg.rank * out_stride + e * (long long)sizeof(T)) = top;
+            }
         }
     }
 }

@@ -134,13 +134,18 @@ int bine_allreduce(const void *sendbuf, void *recvbuf, int count, bine_datatype_
  * (strides from bine_comm_set_layout).  Column windows of ~32 MiB flow
  * through the device on three streams so that the host->device copy of one
  * window, the reduction of the previous one and the device->host copy of
- * the one before that overlap.  Pinned host memory (cudaHostAlloc or
+ * the one before that overlap (window size: bine_comm_set_host_window).  Pinned host memory (cudaHostAlloc or
  * cudaHostRegister) gives full PCIe bandwidth; pageable memory works at
  * pageable-copy speed.  Returns when the result is in `recvbuf`.  Results
  * equal bine_allreduce's (the fused kernels run whatever the engine
  * setting; float sums follow the communicator's float order). */
 int bine_allreduce_host(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
                         bine_comm_t comm);
+
+/* Bytes of one column window of bine_allreduce_host over all ranks
+ * (default 32 MiB; at least 4 KiB).  Smaller windows shorten the pipeline's
+ * fill and drain; larger ones cut per-copy overhead. */
+int bine_comm_set_host_window(bine_comm_t comm, long long window_bytes);
 
 /* MPI_Reduce_scatter, lib/libbine.cc:1064 (recvcounts must all be equal, as
  * the reference's block implementation assumes, lib/libbine.cc:1065). */

@@ -110,6 +110,13 @@ def reference_is_right(case, x):
     ("reduce_scatter", "VEC_HALVING_CONT_PERMUTE", 64, 1024, None, 1),
     ("reduce", "BINOMIAL_TREE", 64, 20_000, None, 1),
     ("reduce", "REDUCE_SCATTER_GATHER", 32, 20_001, None, 1),
+    # Block boundaries off the 16-byte grid: vector bodies plus element
+    # heads and tails.
+    ("allreduce", "B", 96, 50_000, None, 1),
+    ("allreduce", "B_COALESCE", 48, 48 * 777 + 5, None, 2),
+    ("allreduce", "L", 72, 30_001, [6, 12], 2),
+    ("allreduce", "B", 384, 131_072, None, 1),
+    ("allreduce", "B", 1000, 64_007, None, 1),  # programs of 1,000 leaves: over 48 KB of shared memory
 ])
 def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
     sc, _ = buffer_counts(coll, count, P)
@@ -124,6 +131,7 @@ def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
 @pytest.mark.parametrize("lanes", [1, 2, 4, 8])
 @pytest.mark.parametrize("coll,variant,P,count,dims,ports", [
     ("allreduce", "B", 256, 256 * 64, None, 1),
+    ("allreduce", "B", 96, 50_000, None, 1),
     ("allreduce", "B", 96, 96 * 512, None, 1),
     ("allreduce", "B_COALESCE", 48, 48 * 776, None, 2),
     ("allreduce", "L", 64, 50_000, None, 1),
