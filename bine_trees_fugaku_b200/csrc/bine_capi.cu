@@ -501,11 +501,13 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
             K = c->tree_split;
             while (K > 1 && min_leaves < K) K /= 2;
         } else {
-            // Measured on B200: 4 lanes beat 1 and 8 from 2 to 64 MiB per
-            // rank (the one-lane form needs 74 registers, 3 blocks per SM;
-            // the split form 64, 4 blocks), so the automatic choice is 4
-            // wherever every part keeps at least 8 leaves.
-            while (K < 4 && min_leaves >= 16 * K) K *= 2;
+            // By P, as measured on B200 at 2-4 MiB per rank (GB/s for 1 / 2
+            // / 4 / 8 warps per vector group): P = 64: 4649 / 5424 / 5001 /
+            // 4407; P = 96: 3508 / 4566 / 4165 / 3661; P = 256: 5481 / 5843 /
+            // 6026 / 5879; P = 384: 4023 / 4244 / 4216 / 4065; P = 1000:
+            // 2805 / 2825 / 2898 / 3372.
+            const int P = c->P;
+            K = P < 32 ? 1 : (P < 128 ? 2 : (P < 512 ? 4 : 8));
         }
         while (K > 1 && min_leaves < 2 * K) K /= 2;  // 2K parts of at least one leaf
         if (K > 1) {

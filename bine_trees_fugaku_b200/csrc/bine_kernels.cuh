@@ -269,11 +269,17 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
         const TreeTile tile = tiles[t];
         const TreeSeg sg = segs[tile.seg];
         __syncthreads();
-        for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
+        // Staged with each leaf's byte offset (rank row + shift) precomputed.
+        for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) {
+            TreeEntry q = prog[sg.prog_begin + i];
+            q.shift = (long long)q.rank * in_stride + q.shift * (long long)sizeof(T);
+            sprog[i] = q;
+        }
         __syncthreads();
         const long long col = (long long)threadIdx.x * L;
         if (col >= tile.n) continue;
         const long long e = sg.off + tile.start + col;  // output element
+        const char* base = in + e * (long long)sizeof(T);
         uint4 top = make_uint4(0, 0, 0, 0);
         int sp = 0;
         const int len = sg.prog_len;
@@ -283,7 +289,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
         for (int u = 0; u < 8; u++)
             if (u < len) {
                 const TreeEntry q = sprog[u];
-                ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                ring[u] = ld_stream(base + q.shift);
             }
         for (int k0 = 0; k0 < len; k0 += 8) {
 #pragma unroll
@@ -293,7 +299,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_vec(const char* __restrict__ 
                     const uint4 v = ring[u];
                     if (k + 8 < len) {
                         const TreeEntry q = sprog[k + 8];
-                        ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                        ring[u] = ld_stream(base + q.shift);
                     }
                     if (k > 0) stk.set(sp++, top);
                     top = v;
@@ -326,11 +332,12 @@ struct TreeComb {  // combine entry: push part `part`, then `adds` additions
     int32_t part, adds;
 };
 
-// Evaluates program entries [b, b + len) for element `e` (one 16-byte
-// vector), loads kRing entries ahead of the additions.
+// Evaluates program entries [b, b + len) for one 16-byte vector whose first
+// input element is at `base` (entries hold each leaf's byte offset from
+// there), loads kRing entries ahead of the additions.
 template <typename T, bool SMEM, int kRing>
-__device__ __forceinline__ uint4 eval_program(const char* __restrict__ in, long long in_stride, long long e,
-                                              const TreeEntry* sprog, int b, int len, EvalStack<SMEM>& stk) {
+__device__ __forceinline__ uint4 eval_program(const char* __restrict__ base, const TreeEntry* sprog, int b, int len,
+                                              EvalStack<SMEM>& stk) {
     uint4 top = make_uint4(0, 0, 0, 0);
     int sp = 0;
     uint4 ring[kRing];
@@ -338,7 +345,7 @@ __device__ __forceinline__ uint4 eval_program(const char* __restrict__ in, long 
     for (int u = 0; u < kRing; u++)
         if (u < len) {
             const TreeEntry q = sprog[b + u];
-            ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+            ring[u] = ld_stream(base + q.shift);
         }
     for (int k0 = 0; k0 < len; k0 += kRing) {
 #pragma unroll
@@ -348,7 +355,7 @@ __device__ __forceinline__ uint4 eval_program(const char* __restrict__ in, long 
                 const uint4 v = ring[u];
                 if (k + kRing < len) {
                     const TreeEntry q = sprog[b + k + kRing];
-                    ring[u] = ld_stream(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+                    ring[u] = ld_stream(base + q.shift);
                 }
                 if (k > 0) stk.set(sp++, top);
                 top = v;
@@ -391,7 +398,11 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
         const TreeSeg sg = segs[tile.seg];
         __syncthreads();  // the previous tile's partials and program are consumed
         if (tile.seg != cur) {  // block-uniform
-            for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
+            for (int i = threadIdx.x; i < sg.prog_len; i += blockDim.x) {
+                TreeEntry q = prog[sg.prog_begin + i];
+                q.shift = (long long)q.rank * in_stride + q.shift * (long long)sizeof(T);  // byte offset
+                sprog[i] = q;
+            }
             if (threadIdx.x <= nparts) spart[threadIdx.x] = parts[(long long)tile.seg * (nparts + 1) + threadIdx.x];
             if (threadIdx.x < nparts) scomb[threadIdx.x] = comb[(long long)tile.seg * nparts + threadIdx.x];
             if (threadIdx.x < nparts + K + 1)
@@ -405,8 +416,8 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
         if (active) {
             for (int pi = sasg[nparts + j]; pi < sasg[nparts + j + 1]; pi++) {
                 const int p = sasg[pi];
-                partial[g][p][lane] =
-                    eval_program<T, SMEM, 4>(in, in_stride, e, sprog, spart[p], spart[p + 1] - spart[p], stk);
+                partial[g][p][lane] = eval_program<T, SMEM, 4>(in + e * (long long)sizeof(T), sprog, spart[p],
+                                                               spart[p + 1] - spart[p], stk);
             }
         }
         __syncthreads();

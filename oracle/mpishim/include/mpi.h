@@ -84,6 +84,10 @@ int MPI_Comm_rank(MPI_Comm comm, int *rank);
 int MPI_Type_size(MPI_Datatype datatype, int *size);
 int MPI_Op_create(MPI_User_function *fn, int commute, MPI_Op *op);
 int MPI_Barrier(MPI_Comm comm);
+int PMPI_Comm_size(MPI_Comm comm, int *size);
+int PMPI_Comm_rank(MPI_Comm comm, int *rank);
+int PMPI_Type_size(MPI_Datatype datatype, int *size);
+int PMPI_Barrier(MPI_Comm comm);
 
 /* Point to point */
 int MPI_Send(const void *buf, int count, MPI_Datatype dt, int dest, int tag, MPI_Comm comm);

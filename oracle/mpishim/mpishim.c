@@ -278,6 +278,13 @@ int MPI_Barrier(MPI_Comm comm) {
     return MPI_SUCCESS;
 }
 
+/* The PMPI_ names of the calls above (every MPI provides both; a PMPI
+ * interposition layer calls these). */
+int PMPI_Comm_size(MPI_Comm comm, int *size) { return MPI_Comm_size(comm, size); }
+int PMPI_Comm_rank(MPI_Comm comm, int *rank) { return MPI_Comm_rank(comm, rank); }
+int PMPI_Type_size(MPI_Datatype datatype, int *size) { return MPI_Type_size(datatype, size); }
+int PMPI_Barrier(MPI_Comm comm) { return MPI_Barrier(comm); }
+
 /* --------------------------------------------------------- point to point */
 
 static struct shim_msg *arena_alloc(size_t payload) {

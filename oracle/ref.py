@@ -54,9 +54,16 @@ TRACE_DTYPE = np.dtype([("src", np.int32), ("dst", np.int32), ("tag", np.int32),
                         ("bytes", np.uint64)])
 
 
+# The same harness linked against the engine's PMPI layer instead of the
+# reference library (``make -C oracle dropin``).
+DROPIN_PATH = os.path.join(_HERE, "_build", "bine_dropin_run")
+
+
 def run(coll, x, count, *, variant=None, dims=None, ports=1, root=0, family="BINE", distance=None,
-        trace=False, timeout=120.0, shim_timeout=20.0):
-    """Runs the reference on rank-major input x[P, send_count]; returns RefResult."""
+        trace=False, timeout=120.0, shim_timeout=20.0, binary=None, extra_env=None):
+    """Runs the reference (or, with binary=DROPIN_PATH, the engine behind
+    the same MPI entry points) on rank-major input x[P, send_count];
+    returns RefResult."""
     x = np.ascontiguousarray(x)
     P = x.shape[0]
     dt = {np.dtype(v[1]): k for k, v in DTYPES.items()}[x.dtype]
@@ -65,11 +72,12 @@ def run(coll, x, count, *, variant=None, dims=None, ports=1, root=0, family="BIN
     with tempfile.TemporaryDirectory() as td:
         fin, fout, ftr = (os.path.join(td, n) for n in ("in.bin", "out.bin", "trace.bin"))
         x.tofile(fin)
-        cmd = [BIN_PATH, "--coll", coll, "--dtype", DT_ARG[dt], "--count", str(count), "--P", str(P),
+        cmd = [binary or BIN_PATH, "--coll", coll, "--dtype", DT_ARG[dt], "--count", str(count), "--P", str(P),
                "--root", str(root), "--in", fin, "--out", fout, "--timeout", str(shim_timeout)]
         if trace:
             cmd += ["--trace", ftr]
         env = base_env(coll, variant, dims, ports, family, distance)
+        env.update(extra_env or {})
         try:
             p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
         except subprocess.TimeoutExpired as e:
