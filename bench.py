@@ -768,8 +768,8 @@ def run_picker_suite(args):
     """Learned variant picker: measures every valid arm of sampled calls on
     the GPU (STEPS engine times, device link accounting), trains bine_mlp on
     80% of the calls and judges its picks on the held-out 20% against
-    exhaustive search and the fixed rule.  --picker-data reuses a measured
-    dataset instead of measuring."""
+    exhaustive search and the fixed rule.  --picker-data adds measured
+    datasets (with --picker-n 0, no new measurement)."""
     import numpy as np
     import torch
 
@@ -784,19 +784,30 @@ def run_picker_suite(args):
         print(m, file=sys.stderr, flush=True)
 
     t0 = time.time()
-    if args.picker_data:
-        z = np.load(args.picker_data)
-        cfgs = json.loads(str(z["configs"]))
-        T, Lb, valid = z["T"].astype(np.float64), z["Lb"], z["valid"]
-        X = np.array([pk.features(c["coll"], c["P"], c["count"], c["es"], c["dims"]) for c in cfgs], np.float32)
-        te = z["test"]
-    else:
+    # Datasets: measured ones given with --picker-data (comma-separated),
+    # plus --picker-n newly measured calls; each keeps its own held-out 20 %.
+    cfgs, T, Lb, valid, te = [], [], [], [], []
+    for path in [p for p in (args.picker_data or "").split(",") if p]:
+        z = np.load(path)
+        te.extend(int(i) + len(cfgs) for i in z["test"])
+        cfgs += json.loads(str(z["configs"]))
+        T.append(z["T"].astype(np.float64))
+        Lb.append(z["Lb"])
+        valid.append(z["valid"])
+    if args.picker_n > 0:
         configs = pk.sample_configs(args.picker_n, seed=args.picker_seed)
-        cfgs, X, T, Lb, valid = pk.measure(configs, reps=3, time_budget_s=args.picker_budget, log=log)
-        perm = np.random.default_rng(5).permutation(len(cfgs))
-        te = np.sort(perm[: len(cfgs) // 5])
-        np.savez_compressed(os.path.join(out_dir, "picker_dataset.npz"), X=X, T=T.astype(np.float32), Lb=Lb,
-                            valid=valid, test=te, configs=json.dumps(cfgs))
+        c2, _, T2, L2, v2 = pk.measure(configs, reps=3, time_budget_s=args.picker_budget, log=log)
+        perm = np.random.default_rng(5 + args.picker_seed).permutation(len(c2))
+        te.extend(int(i) + len(cfgs) for i in np.sort(perm[: len(c2) // 5]))
+        cfgs += c2
+        T.append(T2)
+        Lb.append(L2)
+        valid.append(v2)
+    T, Lb, valid = np.concatenate(T), np.concatenate(Lb), np.concatenate(valid)
+    te = np.array(sorted(te), np.int64)
+    X = np.array([pk.features(c["coll"], c["P"], c["count"], c["es"], c["dims"]) for c in cfgs], np.float32)
+    np.savez_compressed(os.path.join(out_dir, "picker_dataset.npz"), X=X, T=T.astype(np.float32), Lb=Lb,
+                        valid=valid, test=te, configs=json.dumps(cfgs))
     t_measure = time.time() - t0
     # Noise ceiling: re-time some held-out calls; how often is the first
     # measurement's best arm within 5 % of the second measurement's best?
@@ -877,8 +888,9 @@ def main():
     ap.add_argument("--picker-n", type=int, default=1500)
     ap.add_argument("--picker-seed", type=int, default=11)
     ap.add_argument("--picker-budget", type=float, default=900.0, help="seconds of measurement at most")
-    ap.add_argument("--picker-steps", type=int, default=4000)
-    ap.add_argument("--picker-data", default=None, help="a measured picker_dataset.npz to train on")
+    ap.add_argument("--picker-steps", type=int, default=8000)
+    ap.add_argument("--picker-data", default=None,
+                    help="measured picker_dataset.npz files to train on (comma-separated; --picker-n 0 to measure none)")
     ap.add_argument("--picker-repeat", type=int, default=150, help="held-out calls re-timed for the noise ceiling")
     ap.add_argument("--out", default=None, help="directory for the picker's dataset and weights")
     args = ap.parse_args()

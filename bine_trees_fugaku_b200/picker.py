@@ -293,16 +293,24 @@ def measure(configs, reps=3, time_budget_s=None, log=None):
 
 
 # ------------------------------------------------------------- the model
-def targets(T, Lb, valid, stats=None):
+def targets(T, Lb, valid, stats=None, relative=True):
     """Standardised log2 targets; returns (Y [n, OUT_DIM], mask, stats).
-    `stats` reuses another split's standardisation."""
+    `stats` reuses another split's standardisation.  relative: each call's
+    targets are taken relative to its best arm (log2 time over the fastest,
+    log2 busiest-link bytes over the least), so the model spends no capacity
+    on a call's overall scale, which no pick depends on."""
     n = T.shape[0]
     lt = np.where(valid, np.log2(np.maximum(T, 1e-3)), 0.0)
     ll = np.where(valid, np.log2(np.maximum(Lb, 0.0) + 1.0), 0.0)
+    if relative:
+        any_valid = valid.any(1, keepdims=True)
+        lt = np.where(valid, lt - np.where(any_valid, np.min(np.where(valid, lt, np.inf), 1, keepdims=True), 0), 0.0)
+        ll = np.where(valid, ll - np.where(any_valid, np.min(np.where(valid, ll, np.inf), 1, keepdims=True), 0), 0.0)
     st = stats or {"t_mean": float(lt[valid].mean()), "t_std": float(lt[valid].std() + 1e-9),
                    "l_mean": float(ll[valid].mean()), "l_std": float(ll[valid].std() + 1e-9)}
     Y = np.zeros((n, OUT_DIM), np.float32)
     M = np.zeros((n, OUT_DIM), np.float32)
+    st.setdefault("relative", bool(relative))
     Y[:, :NARMS] = (lt - st["t_mean"]) / st["t_std"]
     Y[:, NARMS:2 * NARMS] = (ll - st["l_mean"]) / st["l_std"]
     M[:, :NARMS] = valid

@@ -100,12 +100,17 @@ def test_targets_mask_invalid_arms():
     T = np.array([[10.0, np.nan] + [np.nan] * (pk.NARMS - 2), [20.0, 40.0] + [np.nan] * (pk.NARMS - 2)])
     Lb = np.where(np.isnan(T), np.nan, 1024.0)
     valid = ~np.isnan(T)
-    Y, M, st = pk.targets(T, Lb, valid)
+    Y, M, st = pk.targets(T, Lb, valid, relative=False)
     assert Y.shape == (2, pk.OUT_DIM) and M.shape == (2, pk.OUT_DIM)
     assert M[0, 0] == 1 and M[0, 1] == 0 and M[1, 1] == 1 and M[:, 2 * pk.NARMS:].sum() == 0
     assert np.all(np.isfinite(Y))
     lt = np.log2([10.0, 20.0, 40.0])
     assert st["t_mean"] == pytest.approx(lt.mean())
+    # Relative targets: each call's best arm is 0 before standardisation
+    # (log2 times 0; 0 and 1), and the ordering within a call is kept.
+    Yr, Mr, sr = pk.targets(T, Lb, valid)
+    assert sr["t_mean"] == pytest.approx(1.0 / 3.0) and sr["relative"]
+    assert Yr[1, 0] < Yr[1, 1] and np.array_equal(Mr, M)
 
 
 def test_evaluate_perfect_and_fixed_rule_arithmetic():
