@@ -5,6 +5,7 @@ import glob
 import os
 import re
 
+import numpy as np
 import pytest
 
 import bine_trees_fugaku_b200 as bine
@@ -52,3 +53,37 @@ def test_unsupported_cases_report_the_reference_line():
     c.set_algo("allreduce", "B")
     with pytest.raises(bine.Unsupported):
         c.plan_stats("allreduce", 5)  # count < ports * P (lib/libbine.cc:1036)
+
+
+def test_collective_argument_errors_are_reported_before_any_device_work():
+    """The checks the reference leaves to asserts (lib/libbine.cc:1035-1036,
+    1170-1171) come back as BINE_ERR_ARG, on a host without a GPU too; a
+    zero count is a no-op that succeeds without touching the device."""
+    c = bine.Comm(8)
+    fake = 1 << 20  # an address never dereferenced: every case fails or returns first
+    err = lambda f: pytest.raises(bine.BineError, match="bine error 1:")  # noqa: E731
+    with err(None):
+        c.allreduce(fake, fake, -1, bine.INT32)
+    with err(None):
+        c.allreduce(fake, fake, 16, 99)
+    with err(None):
+        c.allreduce(fake, fake, 16, bine.INT32, op=1)
+    with err(None):
+        c.reduce(fake, fake, 16, bine.INT32, root=8)
+    with err(None):
+        c.bcast(fake, 16, bine.INT32, -1)
+    with err(None):
+        c.allreduce(None, fake, 16, bine.INT32)
+    c.set_layout(16, 16)  # stride of 16 bytes < 16 int32 per rank
+    with err(None):
+        c.allreduce(fake, fake, 16, bine.INT32)
+    c.set_layout(0, 0)
+    for coll in bine.COLLS:
+        c.run(coll, fake, fake, 0, bine.INT32)  # count 0: nothing to do
+    c.allreduce_host(np.zeros((8, 1), np.int32), np.zeros((8, 1), np.int32), 0, bine.INT32)
+    with err(None):
+        c.set_tree_split(3)
+    with err(None):
+        c.set_host_window(100)
+    with err(None):
+        c.set_segment(-5)

@@ -419,3 +419,28 @@ def test_allreduce_host_pageable_in_place_and_strided():
     comm.allreduce_host(big, out, count, bine.INT32)
     assert np.array_equal(out[:, :count], expected("allreduce", x, P, count))
     assert np.all(out[:, count:] == 7)
+
+
+@pytest.mark.parametrize("engine", ["fused", "steps"])
+@pytest.mark.parametrize("coll", bine.COLLS)
+def test_zero_and_ragged_counts(engine, coll):
+    """count 0 leaves every output byte as it was; counts below P (1 and
+    3 elements per rank) give the MPI result, or, on the engine that follows
+    the reference's schedule, a clean refusal where the reference cannot
+    run them."""
+    P, root = 16, 0
+    comm = make_comm(P, coll, list(bine.VARIANTS[coll])[0], engine=engine)
+    sentinel = torch.full((P, 64), 7, dtype=torch.int32, device="cuda")
+    comm.run(coll, sentinel.clone(), sentinel, 0, bine.INT32, root)
+    comm.synchronize()
+    assert int((sentinel != 7).sum()) == 0
+    for count in (1, 3):
+        sc, _ = buffer_counts(coll, count, P)
+        x = np.random.default_rng(count).integers(-1000, 1001, (P, sc)).astype(np.int32)
+        try:
+            out = run(comm, coll, x, count, root)
+        except bine.Unsupported:
+            assert engine == "steps"
+            continue
+        rr = receiving_ranks(coll, P, root)
+        assert np.array_equal(out[rr], expected(coll, x, P, count, root)[rr])
