@@ -1,8 +1,8 @@
 """The learned picker against exhaustive search and the fixed rule, on the
-committed measurements (tests/golden/picker_dataset.npz: 3,000 sampled
-calls, every valid arm timed on a B200 with the STEPS engine, made by
-`python bench.py --suite picker --picker-n 3000`) and the committed weights trained on the
-80 % of calls outside its `test` split.
+committed measurements (tests/golden/picker_dataset.npz: 6,000 sampled
+calls in two batches, every valid arm timed on a B200 with the STEPS engine,
+made by `python bench.py --suite picker`) and the committed weights trained
+on the 80 % of calls outside its `test` split.
 
 The CPU test evaluates the weights with the float64 reference of the MLP
 (oracle/mlp_ref.py, bf16 rounding at the kernels' points); the GPU test
@@ -20,7 +20,9 @@ from oracle import mlp_ref
 HERE = os.path.dirname(os.path.abspath(__file__))
 DATASET = os.path.join(HERE, "golden", "picker_dataset.npz")
 # The committed dataset: 3,000 sampled calls (bench.py --suite picker
-# --picker-n 3000), every valid arm timed on a B200 with the STEPS engine.
+# --picker-n 3000), then 3,000 more with another seed merged in
+# (--picker-data <first> --picker-n 3000 --picker-seed 12), every valid arm
+# timed on a B200 with the STEPS engine.
 
 
 def load():
@@ -41,13 +43,13 @@ def check_gain(ev):
     # held-out calls, far more often than the fixed rule, and are faster
     # than the fixed rule on average; the model's three best arms, timed,
     # hold an arm within 5 % of the optimum on >= 95 % of the calls.
-    assert ev["held_out_calls"] >= 400
-    assert ev["pick_within_5pct_of_optimum"] >= 0.85
+    assert ev["held_out_calls"] >= 900
+    assert ev["pick_within_5pct_of_optimum"] >= 0.87
     assert ev["pick_within_5pct_of_optimum"] >= ev["fixed_rule_within_5pct_of_optimum"] + 0.4
-    assert ev["pick_time_over_optimum_geomean"] <= 1.04
+    assert ev["pick_time_over_optimum_geomean"] <= 1.03
     assert ev["shortlist3_within_5pct_of_optimum"] >= 0.95
     assert ev["speedup_vs_fixed_rule_geomean"] >= 1.2
-    assert ev["link_bytes_over_minimum_geomean"] <= 1.02
+    assert ev["link_bytes_over_minimum_geomean"] <= 1.01
 
 
 def test_dataset_is_consistent():
@@ -59,7 +61,7 @@ def test_dataset_is_consistent():
         assert np.allclose(X[i], pk.features(c["coll"], c["P"], c["count"], c["es"], c["dims"]))
         for a in np.nonzero(valid[i])[0]:
             assert pk.statically_valid(pk.ARMS[a], c["coll"], c["P"], c["count"], c["dims"])
-    assert len(set(te.tolist())) == len(te) == len(cfgs) // 5
+    assert len(set(te.tolist())) == len(te) == len(cfgs) // 5 and te.max() < len(cfgs)
 
 
 def test_learned_picks_beat_the_fixed_rule_on_held_out_calls():
