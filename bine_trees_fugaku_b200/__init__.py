@@ -23,7 +23,7 @@ SUM = 0
 SUCCESS, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_INTERNAL = range(7)
 ENGINE_FUSED, ENGINE_STEPS = 0, 1
 ORDER_REFERENCE, ORDER_FAST = 0, 1
-FAMILY = {"BINE": 1, "RECDOUB": 2}
+FAMILY = {"BINE": 1, "RECDOUB": 2, "BRUCK": 3}
 DISTANCE = {None: -1, "INCREASING": 0, "DECREASING": 1}
 
 COLLS = ["allreduce", "reduce_scatter", "allgather", "bcast", "reduce", "alltoall", "scatter", "gather"]

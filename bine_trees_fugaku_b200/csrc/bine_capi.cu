@@ -1504,7 +1504,10 @@ int bine_comm_set_ports(bine_comm_t comm, int ports) {
 int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int family, int distance) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     if ((int)coll < 0 || (int)coll >= kNumColls) return fail(BINE_ERR_ARG, "invalid collective");
-    if (family != BINE_FAMILY_BINE && family != BINE_FAMILY_RECDOUB) return fail(BINE_ERR_ARG, "invalid family");
+    if (family != BINE_FAMILY_BINE && family != BINE_FAMILY_RECDOUB && family != BINE_FAMILY_BRUCK)
+        return fail(BINE_ERR_ARG, "invalid family");
+    if (family == BINE_FAMILY_BRUCK && coll != BINE_COLL_ALLTOALL)
+        return fail(BINE_ERR_ARG, "the BRUCK family is an alltoall algorithm");
     if (distance != BINE_DISTANCE_DEFAULT && distance != kIncreasing && distance != kDecreasing)
         return fail(BINE_ERR_ARG, "invalid distance");
     static const int valid[kNumColls][4] = {{kArL, kArB, kArBCont, kArBCoalesce},

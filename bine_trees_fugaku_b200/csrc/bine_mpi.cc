@@ -155,7 +155,10 @@ int make_comm() {
         if (variant < 0) continue;  // a name of the reference's other layers: keep the default
         snprintf(key, sizeof key, "LIBBINE_%s_ALGO_FAMILY", kCollEnv[c]);
         const char* fam = env(key);
-        const int family = fam && strcmp(fam, "RECDOUB") == 0 ? BINE_FAMILY_RECDOUB : BINE_FAMILY_BINE;
+        const int family = !fam ? BINE_FAMILY_BINE
+                           : strcmp(fam, "RECDOUB") == 0 ? BINE_FAMILY_RECDOUB
+                           : strcmp(fam, "BRUCK") == 0 && c == BINE_COLL_ALLTOALL ? BINE_FAMILY_BRUCK
+                                                                                 : BINE_FAMILY_BINE;
         snprintf(key, sizeof key, "LIBBINE_%s_DISTANCE", kCollEnv[c]);
         const char* dist = env(key);
         const int distance = !dist ? BINE_DISTANCE_DEFAULT

@@ -1065,6 +1065,53 @@ void gen_alltoall(const Gen& g) {
     b.finish(g.s);
 }
 
+// Bruck's log-step alltoall, the reference's comparator (bruck_alltoall,
+// lib/libbine_coll_alltoall.cc:18-107): rotate the blocks by the rank, then
+// at step k = 1, 2, 4, ... pack the blocks whose index has bit k set,
+// exchange them with rank + k / rank - k in one message and unpack them in
+// place, and finally rotate back into recvbuf.  Any P.  Workspace: the
+// rotated blocks [0, P*c), the outgoing pack and the incoming pack
+// ((P+1)/2 blocks each), as the reference's three temporary buffers.
+void gen_alltoall_bruck(const Gen& g) {
+    const int P = g.P;
+    const int64_t c = g.k.count;
+    const int64_t half = (P + 1) / 2;
+    g.s->send_elems = g.s->recv_elems = c * P;
+    const int64_t pack = (int64_t)P * c, inbox = pack + half * c;
+    Builder b(P, inbox + half * c);
+    b.begin();
+    for (int r = 0; r < P; r++)
+        for (int i = 0; i < P; i++) b.copy(R(r, kBufTmp, pmod(i - r, P) * c), R(r, kBufSend, (int64_t)i * c), c);
+    b.end(g.s);
+    for (int k = 1; k < P; k <<= 1) {
+        std::vector<int> idx;
+        for (int i = k; i < P; i++)
+            if (i & k) idx.push_back(i);
+        const int64_t n = (int64_t)idx.size() * c;
+        b.begin();
+        for (int r = 0; r < P; r++)
+            for (size_t j = 0; j < idx.size(); j++)
+                b.copy(R(r, kBufTmp, pack + (int64_t)j * c), R(r, kBufTmp, (int64_t)idx[j] * c), c);
+        b.end(g.s);
+        b.begin();
+        for (int r = 0; r < P; r++) {
+            b.send(r, (r + k) % P, 0, R(r, kBufTmp, pack), n);
+            b.recv(r, pmod(r - k, P), 0, R(r, kBufTmp, inbox), n);
+        }
+        b.end(g.s);
+        b.begin();
+        for (int r = 0; r < P; r++)
+            for (size_t j = 0; j < idx.size(); j++)
+                b.copy(R(r, kBufTmp, (int64_t)idx[j] * c), R(r, kBufTmp, inbox + (int64_t)j * c), c);
+        b.end(g.s);
+    }
+    b.begin();
+    for (int r = 0; r < P; r++)
+        for (int i = 0; i < P; i++) b.copy(R(r, kBufRecv, pmod(r - i, P) * c), R(r, kBufTmp, (int64_t)i * c), c);
+    b.end(g.s);
+    b.finish(g.s);
+}
+
 // Scatter down a negabinary binomial tree with wrap-around block ranges
 // (bine_scatter_mpi, lib/libbine_coll_scatter.cc:187-324).  Interior ranks
 // keep the blocks of their subtree in the workspace.
@@ -1429,6 +1476,8 @@ bool Planner::build(const PlanKey& k, Schedule* out, std::string* err) const {
     try {
         if (k.ports < 1 || k.ports > kMaxPorts) throw PlanError("ports must be in [1, 6] (lib/libbine.cc:98)");
         if (k.root < 0 || k.root >= t_.size) throw PlanError("root out of range");
+        if (k.family == kFamilyBruck && k.coll != kAlltoall)
+            throw PlanError("the BRUCK family exists for alltoall only; the other entry points assert on it (e.g. lib/libbine.cc:1059, 1146, 1247)");
         switch (k.coll) {
         case kAllreduce:
             if (k.variant == kArL) gen_allreduce_l(g);
@@ -1449,7 +1498,10 @@ bool Planner::build(const PlanKey& k, Schedule* out, std::string* err) const {
             if (k.variant == kRdRedscatGather) gen_reduce_redscat_gather(g);
             else gen_reduce_tree(g);
             break;
-        case kAlltoall: gen_alltoall(g); break;
+        case kAlltoall:
+            if (k.family == kFamilyBruck) gen_alltoall_bruck(g);
+            else gen_alltoall(g);
+            break;
         case kScatter: gen_scatter(g); break;
         case kGather: gen_gather(g); break;
         default: throw PlanError("unknown collective");

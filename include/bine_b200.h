@@ -74,7 +74,9 @@ enum {
 };
 
 /* LIBBINE_<COLL>_ALGO_FAMILY and LIBBINE_<COLL>_DISTANCE. */
-enum { BINE_FAMILY_BINE = 1, BINE_FAMILY_RECDOUB = 2 };
+/* LIBBINE_<COLL>_ALGO_FAMILY (lib/libbine_common.h:77-85).  BRUCK is the
+ * reference's comparator for alltoall (lib/libbine_coll_alltoall.cc:18). */
+enum { BINE_FAMILY_BINE = 1, BINE_FAMILY_RECDOUB = 2, BINE_FAMILY_BRUCK = 3 };
 enum { BINE_DISTANCE_INCREASING = 0, BINE_DISTANCE_DECREASING = 1, BINE_DISTANCE_DEFAULT = -1 };
 
 /* Execution engines.

@@ -1251,6 +1251,27 @@ void alltoall_log(const Ctx& c, int r) {
     }
 }
 
+// bruck_alltoall (lib/libbine_coll_alltoall.cc:18-107): rotate, log2(P)
+// packed exchanges with rank + k / rank - k, rotate back.  Any P.
+void alltoall_bruck(const Ctx& c, int r) {
+    const int size = c.P;
+    const size_t cb = (size_t)c.count * c.es;
+    const size_t half = (size_t)(size + 1) / 2;
+    char* recvbuf = out_of(c, r);
+    std::vector<char> tsend(cb * size + 1, 0), tbuf(cb * half + 1), trecv(cb * half + 1);
+    for (int i = 0; i < size; i++) std::memcpy(tsend.data() + (size_t)mod(i - r, size) * cb, in_of(c, r) + i * cb, cb);
+    for (int k = 1; k < size; k <<= 1) {
+        std::vector<int> idx;
+        for (int i = k; i < size; i++)
+            if (i & k) idx.push_back(i);
+        for (size_t j = 0; j < idx.size(); j++) std::memcpy(tbuf.data() + j * cb, tsend.data() + idx[j] * cb, cb);
+        c.world->send(r, mod(r + k, size), 0, tbuf.data(), idx.size() * cb);
+        c.world->recv(r, mod(r - k, size), 0, trecv.data(), idx.size() * cb);
+        for (size_t j = 0; j < idx.size(); j++) std::memcpy(tsend.data() + idx[j] * cb, trecv.data() + j * cb, cb);
+    }
+    for (int i = 0; i < size; i++) std::memcpy(recvbuf + (size_t)mod(r - i, size) * cb, tsend.data() + i * cb, cb);
+}
+
 // ----------------------------------------------------------- scatter/gather
 // bine_scatter_mpi (lib/libbine_coll_scatter.cc:187-324).
 void scatter_tree(const Ctx& c, int r) {
@@ -1557,7 +1578,10 @@ int oracle_run(const oracle_call_t* call, const void* in, void* out, oracle_msg_
             else
                 body = [&](int r) { reduce_tree(c, r); };
             break;
-        case OR_ALLTOALL: body = [&](int r) { alltoall_log(c, r); }; break;
+        case OR_ALLTOALL:
+            if (call->family == OR_FAMILY_BRUCK) body = [&](int r) { alltoall_bruck(c, r); };
+            else body = [&](int r) { alltoall_log(c, r); };
+            break;
         case OR_SCATTER:
             if (c.count < c.ports) throw Unsupported("scatter asserts recvcount >= ports (lib/libbine.cc:1331)");
             body = [&](int r) { scatter_tree(c, r); };

@@ -38,6 +38,11 @@ def _cases():
         out.append({"coll": coll, "variant": var, "P": 16, "root": 5, "dtype": "float", "count": 9, "seed": 11})
     for coll, var in (("reduce_scatter", "VEC_HALVING_CONT_PERMUTE"), ("allgather", "VEC_DOUBLING_CONT_PERMUTE")):
         out.append({"coll": coll, "variant": var, "P": 16, "ports": 3, "dtype": "int32", "count": 7, "seed": 5})
+    # Bruck's alltoall, the reference's comparator (any P).
+    for P in (4, 8, 16, 6, 12):
+        for dt in ("int32", "float"):
+            out.append({"coll": "alltoall", "variant": "LOG", "P": P, "family": "BRUCK", "dtype": dt, "count": 5,
+                        "seed": 2000 + P})
     return out
 
 
