@@ -659,12 +659,43 @@ def run_sweep_suite(args):
         for sk in skipped:
             f.write(json.dumps(dict(sk, skipped="device working set above 80% of free HBM")) + "\n")
     timed = [r for r in rows if "us" in r]
+    # The reference library itself at a sample of the points (P = 16 and
+    # 64, float32, three sizes, its default variants; host memory bounded),
+    # timed as bench.cc times it, next to the fused engine at the same point.
+    refs = []
+    if args.sweep_reference:
+        from oracle import ref
+
+        fused = {(r["coll"], r["P"], r["bytes_per_rank"], r["dtype"]): r for r in timed if r["engine"] == "fused"}
+        with open(os.path.join(out_dir, "sweep_reference.jsonl"), "w") as f:
+            for P in (16, 64):
+                for coll in SWEEP_COLLS:
+                    for nbytes in (32, 32 * 4 ** 5, 32 * 4 ** 8):
+                        count = max(1, nbytes // 4)
+                        se, re = bine.row_counts(coll, count, P)
+                        if (se + re) * 4 > 16 << 20:
+                            continue
+                        j = ref.time_collective(coll, "float", count, P, iters=5, warmup=2, timeout=120)
+                        e = fused.get((coll, P, count * 4, "float32"))
+                        r = {"coll": coll, "P": P, "bytes_per_rank": count * 4, "dtype": "float32",
+                             "ref_ok": bool(j.get("ok")), "cores": os.cpu_count()}
+                        if j.get("ok"):
+                            ab = sweep_algo_bytes(coll, P, count, 4)
+                            r.update(ref_us=j["median_s"] * 1e6, ref_gbs=ab / j["median_s"] / 1e9)
+                            if e:
+                                r.update(engine_us=e["us"], speedup=j["median_s"] * 1e6 / e["us"])
+                        refs.append(r)
+                        f.write(json.dumps(r) + "\n")
     best = {}
     for r in timed:
         k = (r["coll"], r["engine"])
         if k not in best or r["algo_gbs"] > best[k]["algo_gbs"]:
             best[k] = r
     line = {"suite": "sweep", "points_timed": len(timed), "points_incorrect": len(bad),
+            "reference_points": len([r for r in refs if "speedup" in r]),
+            "speedup_over_reference_range": [round(min(r["speedup"] for r in refs if "speedup" in r), 1),
+                                             round(max(r["speedup"] for r in refs if "speedup" in r), 1)]
+            if any("speedup" in r for r in refs) else None,
             "points_unsupported": len([r for r in rows if "unsupported" in r]), "points_skipped": len(skipped),
             "best_algo_gbs": {f"{k[0]}/{k[1]}": round(v["algo_gbs"], 1) for k, v in sorted(best.items())},
             "seconds": round(time.time() - t_start, 1), "jsonl": os.path.relpath(path, ROOT)}
@@ -885,6 +916,8 @@ def main():
                     help="lanes per output vector of the exact-order float kernel (0: chosen per call)")
     ap.add_argument("--suite", default="headline", choices=["headline", "batch", "picker", "sweep", "links"])
     ap.add_argument("--batch-n", type=int, default=4096)
+    ap.add_argument("--sweep-reference", action="store_true",
+                    help="also time the reference library at a sample of the sweep's points")
     ap.add_argument("--picker-n", type=int, default=1500)
     ap.add_argument("--picker-seed", type=int, default=11)
     ap.add_argument("--picker-budget", type=float, default=900.0, help="seconds of measurement at most")
