@@ -617,9 +617,13 @@ unsigned resident_blocks(bine_comm_t c, K kern, int threads, size_t smem) {
 template <typename T, int COLS>
 int launch_sum_cols(bine_comm_t c, int mode, const char* in, long long ist, char* out, long long ost, int P,
                     long long ncol, long long blk_vec, int root) {
+    // One tile per block, up to 64 blocks per SM (then grid-stride): the
+    // hardware scheduler back-fills SMs as blocks finish, where a single
+    // resident wave walking the tiles leaves a tail (measured on B200, P =
+    // 256, 4 MiB per rank: 5716 GB/s resident wave, 6347 one tile per
+    // block).
     const long long tiles = (ncol + COLS - 1) / COLS;
-    const unsigned g = (unsigned)std::min<long long>(
-        tiles, resident_blocks(c, dev::k_sum_vec<T, dev::kSumAllreduce, COLS>, dev::kThreads, 0));
+    const unsigned g = (unsigned)std::min<long long>(tiles, 64LL * std::max(1, c->num_sms));
     if (mode == dev::kSumAllreduce)
         dev::k_sum_vec<T, dev::kSumAllreduce, COLS><<<g, dev::kThreads, 0, c->stream>>>(in, ist, out, ost, P, ncol,
                                                                                          blk_vec, root);
@@ -645,9 +649,13 @@ int launch_sum(bine_comm_t c, int mode, const char* in, long long ist, char* out
         const long long ncol = elems * es / 16;
         if (ncol > 0) {
             const long long blk_vec = mode == dev::kSumReduceScatter ? blk * es / 16 : 0;
-            // Row groups of at least 8 rows: 1 group up to P = 15, 2 up to
-            // 31, 4 up to 63, 8 beyond (tile widths 256 / 128 / 64 / 32).
-            const int cols = P < 16 ? 256 : (P < 32 ? 128 : (P < 64 ? 64 : 32));
+            // Tiles of 64 columns (4 row groups), or 256 (one group) below
+            // P = 16; narrower while a call would have fewer than two tiles
+            // per SM.  Measured on B200 at 4 MiB per rank (GB/s, old rule ->
+            // 64 columns): P = 16: 6406 -> 7084; 64: 5726 -> 6194; 256: 5716
+            // -> 6347; 1024: 5751 -> 6316.
+            int cols = P < 16 ? 256 : 64;
+            while (cols > 32 && ncol / cols < 2LL * std::max(1, c->num_sms)) cols /= 2;
             int rc;
             switch (cols) {
             case 256: rc = launch_sum_cols<T, 256>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;

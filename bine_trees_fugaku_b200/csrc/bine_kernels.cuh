@@ -121,11 +121,11 @@ enum SumMode { kSumAllreduce = 0, kSumReduceScatter = 1, kSumReduce = 2 };
 // split the P rows of a tile (group g sums rows [g*P/G, (g+1)*P/G) of its
 // lane's column, 8 loads in flight per thread), the partial sums meet in
 // shared memory, and all threads then store the result rows.  The host
-// picks COLS from P so that every group has at least 8 rows (wide tiles
-// for small P, 32 columns and 8 groups from P = 64).  Tiles are handed out
-// grid-stride over the resident blocks, so the load balances across the
-// 148 SMs with no wave tail.  `ncol` vector columns per input row;
-// reduce_scatter: `blk` vector columns per destination rank.
+// picks COLS (64 columns and 4 row groups; one group below P = 16; narrower
+// tiles for calls too small to give every SM two tiles) and launches one
+// block per tile up to 64 blocks per SM, beyond which blocks walk the tiles
+// grid-stride.  `ncol` vector columns per input row; reduce_scatter: `blk`
+// vector columns per destination rank.
 constexpr int kSumCols = 32;  // the narrowest tile
 
 template <typename T, int MODE, int COLS>
