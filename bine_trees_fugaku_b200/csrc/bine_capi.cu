@@ -96,6 +96,10 @@ struct DevTrees {
     int* sparts = nullptr;
     dev::TreeComb* scomb = nullptr;
     int* sassign = nullptr;  // per segment: 2K part indices by warp, then K + 1 offsets
+    // One-part plan of every segment (offsets {0, len}, combine {part 0}) for
+    // the staged kernel when there is no split plan.
+    int* uparts = nullptr;
+    dev::TreeComb* ucomb = nullptr;
     dev::TreeTile* stiles = nullptr;
     int nstiles = 0;
     int smax_prog_len = 0;
@@ -124,6 +128,8 @@ struct DevTrees {
         cudaFree(sparts);
         cudaFree(scomb);
         cudaFree(sassign);
+        cudaFree(uparts);
+        cudaFree(ucomb);
         cudaFree(stiles);
     }
 };
@@ -480,7 +486,17 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
     d->h_htiles = htiles;
     d->h_atiles = atiles;
     for (const OutSegment& sg : tp.segs) d->h_seg_off.push_back(sg.off);
-    cudaError_t e1, e2, e3, e4, e5, e6;
+    std::vector<int> uparts;
+    std::vector<dev::TreeComb> ucomb;
+    for (const OutSegment& sg : tp.segs) {
+        uparts.push_back(0);
+        uparts.push_back(sg.prog_len);
+        ucomb.push_back(dev::TreeComb{0, 0});
+    }
+    cudaError_t e1, e2, e3, e4, e5, e6, e7, e8;
+    fill(&d->uparts, uparts, &e7);
+    fill(&d->ucomb, ucomb, &e8);
+    if (e7 != cudaSuccess || e8 != cudaSuccess) return fail(BINE_ERR_CUDA, "uploading the reduction trees failed");
     fill(&d->segs, segs, &e1);
     fill(&d->prog, prog, &e2);
     fill(&d->tiles, tiles, &e3);
@@ -775,12 +791,19 @@ int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist,
         CUDA_TRY(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
         es = c->side;
         if (ts.n[3] > 0) {
-            const size_t prog = (size_t)std::max(1, d.max_prog_len) * sizeof(dev::TreeEntry);
-            const size_t smem = prog + (size_t)(16 / sizeof(T) - 1) * std::max(1, d.max_prog_len) * sizeof(T);
+            // The split plan's parts when there is one (its segments index
+            // the same output runs), else each whole tree as one part.
+            const bool split = d.split_k > 1;
+            if (split && d.split_parts > dev::kMaxParts) return fail(BINE_ERR_INTERNAL, "too many tree parts");
+            const int plen = std::max(1, split ? d.smax_prog_len : d.max_prog_len);
+            const size_t prog = (size_t)plen * sizeof(dev::TreeEntry);
+            const size_t smem = prog + (size_t)(16 / sizeof(T) - 1) * plen * sizeof(T);
             rc = launch_tree_kernel(c, dev::k_tree_staged<T>, smem, ts.n[3], &g);
             if (rc) return rc;
-            dev::k_tree_staged<T><<<g, dev::kThreads, smem, es>>>(in, ist, out, ost, c->P, d.segs, d.prog, ts.t[3],
-                                                                  ts.n[3], (int)(prog / 16));
+            dev::k_tree_staged<T><<<g, dev::kThreads, smem, es>>>(
+                in, ist, out, ost, c->P, split ? d.ssegs : d.segs, split ? d.sprog : d.prog,
+                split ? d.sparts : d.uparts, split ? d.scomb : d.ucomb, split ? d.split_parts : 1, ts.t[3], ts.n[3],
+                (int)(prog / 16));
             CUDA_TRY(cudaGetLastError());
         }
     }

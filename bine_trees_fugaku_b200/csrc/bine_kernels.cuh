@@ -439,51 +439,84 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
 }
 
 // Element form for the short head and tail pieces of segments (fewer
-// elements than one 16-byte vector): the block first loads every leaf value
-// of the tile's elements into shared memory in one parallel round, then
-// one thread per element evaluates the program from there.  The leaf loads
-// of a program are thus issued together instead of one after another.
+// elements than one 16-byte vector).  Per tile the block
+//   1. loads every leaf value of the tile's elements into shared memory in
+//      one parallel round;
+//   2. evaluates the tree's parts (the split plan's `nparts` subtrees, or
+//      the whole tree as one part) with one thread per (element, part);
+//   3. combines each element's partials in the tree's order;
+//   4. spreads the P destination stores over all its threads.
+// Without steps 2 and 4 one thread per element ran the whole P-leaf
+// program and issued all P stores, which made this small kernel as long as
+// the vector kernel beside it at P = 1000.
+constexpr int kMaxParts = 16;
+constexpr int kMaxPiece = 4;  // elements of a piece: fewer than one vector
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_tree_staged(const char* __restrict__ in, long long in_stride,
                                                           char* __restrict__ out, long long out_stride, int P,
                                                           const TreeSeg* __restrict__ segs,
                                                           const TreeEntry* __restrict__ prog,
+                                                          const int* __restrict__ parts,
+                                                          const TreeComb* __restrict__ comb, int nparts,
                                                           const TreeTile* __restrict__ tiles, int ntiles,
                                                           int vals_off) {
     extern __shared__ uint4 sdyn[];
     TreeEntry* sprog = reinterpret_cast<TreeEntry*>(sdyn);
     T* vals = reinterpret_cast<T*>(sdyn + vals_off);
+    __shared__ int spart[kMaxParts + 1];
+    __shared__ TreeComb scomb[kMaxParts];
+    __shared__ T partial[kMaxPiece][kMaxParts];
+    __shared__ T res[kMaxPiece];
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const TreeTile tile = tiles[t];
         const TreeSeg sg = segs[tile.seg];
-        const int len = sg.prog_len;
-        __syncthreads();
+        const int len = sg.prog_len, n = (int)tile.n;
+        __syncthreads();  // the previous tile's values and results are consumed
         for (int i = threadIdx.x; i < len; i += blockDim.x) sprog[i] = prog[sg.prog_begin + i];
+        if (threadIdx.x <= nparts) spart[threadIdx.x] = parts[(long long)tile.seg * (nparts + 1) + threadIdx.x];
+        if (threadIdx.x < nparts) scomb[threadIdx.x] = comb[(long long)tile.seg * nparts + threadIdx.x];
         __syncthreads();
-        const int total = (int)tile.n * len;
-        for (int i = threadIdx.x; i < total; i += blockDim.x) {
-            const int j = i / len, k = i - j * len;
+        const long long e0 = sg.off + tile.start;
+        for (int i = threadIdx.x; i < n * len; i += blockDim.x) {
+            const int jj = i / len, k = i - jj * len;
             const TreeEntry q = sprog[k];
-            const long long e = sg.off + tile.start + j;
-            vals[i] = *(const T*)(in + (long long)q.rank * in_stride + (e + q.shift) * (long long)sizeof(T));
+            vals[i] = *(const T*)(in + (long long)q.rank * in_stride + (e0 + jj + q.shift) * (long long)sizeof(T));
         }
         __syncthreads();
-        if (threadIdx.x < tile.n) {
-            const int j = threadIdx.x;
-            const long long e = sg.off + tile.start + j;
+        for (int w = threadIdx.x; w < n * nparts; w += blockDim.x) {
+            const int jj = w / nparts, p = w - jj * nparts;
+            const T* v = vals + jj * len;
             T stk[kMaxTreeDepth];
             T top = (T)0;
             int sp = 0;
-            for (int k = 0; k < len; k++) {
-                if (k > 0) stk[sp++] = top;
-                top = vals[j * len + k];
+            for (int k = spart[p]; k < spart[p + 1]; k++) {
+                if (k > spart[p]) stk[sp++] = top;
+                top = v[k];
                 for (int a = sprog[k].adds; a > 0; a--) top = add_exact<T>(stk[--sp], top);
             }
-            if (sg.rank < 0) {
-                for (int d = 0; d < P; d++) *(T*)(out + (long long)d * out_stride + e * (long long)sizeof(T)) = top;
-            } else {
-                *(T*)(out + (long long)sg.rank * out_stride + e * (long long)sizeof(T)) = top;
+            partial[jj][p] = top;
+        }
+        __syncthreads();
+        if (threadIdx.x < n) {
+            T stk[kMaxParts];
+            T top = (T)0;
+            int sp = 0;
+            for (int q = 0; q < nparts; q++) {
+                if (q > 0) stk[sp++] = top;
+                top = partial[threadIdx.x][scomb[q].part];
+                for (int a = scomb[q].adds; a > 0; a--) top = add_exact<T>(stk[--sp], top);
             }
+            res[threadIdx.x] = top;
+        }
+        __syncthreads();
+        if (sg.rank < 0) {
+            for (int w = threadIdx.x; w < P * n; w += blockDim.x) {
+                const int d = w / n, jj = w - d * n;
+                *(T*)(out + (long long)d * out_stride + (e0 + jj) * (long long)sizeof(T)) = res[jj];
+            }
+        } else if (threadIdx.x < n) {
+            *(T*)(out + (long long)sg.rank * out_stride + (e0 + threadIdx.x) * (long long)sizeof(T)) = res[threadIdx.x];
         }
     }
 }
