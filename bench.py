@@ -703,6 +703,41 @@ def run_sweep_suite(args):
     return 0 if not bad else 1
 
 
+def run_dropin_suite(args):
+    """Unmodified MPI callers: the oracle's harness (P forked ranks calling
+    MPI_Allreduce on host buffers, timed as bench.cc times it: two
+    barriers, wall time around one call, max over ranks, median) linked
+    against the reference library and, unchanged, against the engine's PMPI
+    layer.  Same workload as the headline line."""
+    from oracle import ref
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "dropin"], check=True, capture_output=True)
+    out = {}
+    for name, binary in (("reference", ref.BIN_PATH), ("engine_pmpi", ref.DROPIN_PATH)):
+        if not os.path.exists(binary):
+            out[name] = {"unavailable": f"{os.path.relpath(binary, ROOT)} is not built"}
+            continue
+        j = ref.time_collective("allreduce", "int32", COUNT, P_RANKS, iters=min(args.steps, 10),
+                                warmup=min(args.warmup, 3), timeout=900, binary=binary)
+        if not j.get("ok"):
+            out[name] = {"error": json.dumps(j)[:300]}
+            continue
+        out[name] = {"median_s": j["median_s"], "gbs": ALGO_BYTES / j["median_s"] / 1e9}
+    line = {"suite": "dropin", "metric": "MPI_Allreduce through the reference's own entry point, host buffers",
+            "unit": "GB/s (algorithmic)", **out, "cores": os.cpu_count(),
+            "config": {"workload": WORKLOAD, "P": P_RANKS, "count_per_rank": COUNT,
+                       "harness": "oracle/ref_harness.cc: P forked ranks, bench.cc timing",
+                       "engine": "PMPI layer: rows gathered in node-shared pinned memory, "
+                                 "bine_allreduce_host pipeline, rows scattered back"}}
+    if "gbs" in out.get("reference", {}) and "gbs" in out.get("engine_pmpi", {}):
+        line["speedup"] = out["engine_pmpi"]["gbs"] / out["reference"]["gbs"]
+    print(json.dumps(line))
+    return 0
+
+
 LINK_TORI = [[2, 2, 2], [4, 4, 4], [8, 8, 8], [64, 64], [32, 256]]
 LINK_SCHEDULES = [("allreduce", "B"), ("allreduce", "L"), ("allgather", "VEC_DOUBLING_CONT_PERMUTE")]
 
@@ -914,7 +949,7 @@ def main():
                     help="column-window bytes of the host-buffer pipeline (e2e leg)")
     ap.add_argument("--tree-split", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="lanes per output vector of the exact-order float kernel (0: chosen per call)")
-    ap.add_argument("--suite", default="headline", choices=["headline", "batch", "picker", "sweep", "links"])
+    ap.add_argument("--suite", default="headline", choices=["headline", "batch", "picker", "sweep", "links", "dropin"])
     ap.add_argument("--batch-n", type=int, default=4096)
     ap.add_argument("--sweep-reference", action="store_true",
                     help="also time the reference library at a sample of the sweep's points")
@@ -936,6 +971,8 @@ def main():
         return run_sweep_suite(args)
     if args.suite == "links":
         return run_links_suite(args)
+    if args.suite == "dropin":
+        return run_dropin_suite(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

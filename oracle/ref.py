@@ -92,9 +92,11 @@ def run(coll, x, count, *, variant=None, dims=None, ports=1, root=0, family="BIN
 
 
 def time_collective(coll, dtype, count, P, *, iters=10, warmup=10, variant=None, dims=None, ports=1, root=0,
-                    timeout=600.0):
-    """Times the reference as bench/bench.cc does; returns the harness JSON."""
-    cmd = [BIN_PATH, "--coll", coll, "--dtype", DT_ARG[dtype], "--count", str(count), "--P", str(P),
+                    timeout=600.0, binary=None):
+    """Times the reference (or, with binary=DROPIN_PATH, the engine behind
+    the same MPI entry points) as bench/bench.cc does; returns the harness
+    JSON."""
+    cmd = [binary or BIN_PATH, "--coll", coll, "--dtype", DT_ARG[dtype], "--count", str(count), "--P", str(P),
            "--root", str(root), "--gen", "uniform", "--iters", str(iters), "--warmup", str(warmup),
            "--timeout", str(timeout)]
     p = subprocess.run(cmd, capture_output=True, text=True, env=base_env(coll, variant, dims, ports),
