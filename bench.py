@@ -899,30 +899,40 @@ def run_picker_suite(args):
     Y, M, st = pk.targets(T[tr], Lb[tr], valid[tr])
     Yv, Mv, _ = pk.targets(T[va], Lb[va], valid[va], st)
     t1 = time.time()
-    mlp, losses = pk.train(X[tr], Y, M, steps=args.picker_steps, log=log, val=(X[va], Yv, Mv))
+    mlps, losses = [], None
+    for seed in range(args.picker_ensemble):
+        m, lo = pk.train(X[tr], Y, M, steps=args.picker_steps, log=log, val=(X[va], Yv, Mv), seed=seed)
+        mlps.append(m)
+        losses = losses or lo
     torch.cuda.synchronize()
     t_train = time.time() - t1
-    pred = pk.predict(mlp, X[te])
+    single = pk.evaluate(pk.predict(mlps[0], X[te]), T[te], Lb[te], valid[te], [cfgs[i] for i in te])
+    pred = pk.predict(mlps, X[te])
     ev = pk.evaluate(pred, T[te], Lb[te], valid[te], [cfgs[i] for i in te])
-    # Pick latency: one forward pass of a 16-row batch, device-timed.
+    # Pick latency: one forward pass of a 16-row batch through every model
+    # of the ensemble, device-timed.
     x16 = torch.from_numpy(X[:16].copy() if len(X) >= 16 else np.zeros((16, pk.IN_DIM), np.float32)).cuda()
     for _ in range(5):
-        mlp.forward(x16)
+        for m in mlps:
+            m.forward(x16)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(100):
-        mlp.forward(x16)
+        for m in mlps:
+            m.forward(x16)
     e1.record()
     torch.cuda.synchronize()
     meta = {"calls": len(cfgs), "held_out": int(len(te)), "train_steps": args.picker_steps,
+            "single_model_pick_within_5pct": single["pick_within_5pct_of_optimum"],
             "device": torch.cuda.get_device_name(0)}
-    pk.save(os.path.join(out_dir, "picker_weights.npz"), mlp, st, meta)
+    pk.save(os.path.join(out_dir, "picker_weights.npz"), mlps, st, meta)
     line = {"suite": "picker", "metric": "learned pick vs exhaustive search (held-out calls)",
-            **ev, "noise_ceiling": ceiling, "calls_measured": len(cfgs), "arms": pk.NARMS,
+            **ev, "models": len(mlps), "single_model_pick_within_5pct": single["pick_within_5pct_of_optimum"],
+            "noise_ceiling": ceiling, "calls_measured": len(cfgs), "arms": pk.NARMS,
             "valid_arms_per_call_mean": float(valid.sum(1).mean()) if len(cfgs) else 0.0,
             "train_loss_first_last": [losses[0], float(np.mean(losses[-50:]))],
             "measure_s": t_measure, "train_s": t_train, "forward16_us": e0.elapsed_time(e1) * 10.0,
-            "config": {"model": "bine_mlp 16-256-256-256-%d GELU, bf16 weights, fp32 accumulate" % pk.OUT_DIM,
+            "config": {"model": "ensemble of bine_mlp 16-256-256-256-%d GELU, bf16 weights, fp32 accumulate" % pk.OUT_DIM,
                        "engine": "steps", "timing": "per arm: median of 3 CUDA-event batches of back-to-back "
                                                     "launches (each batch ~300 us, at most 32 launches)",
                        "calls": "sampled: 60% allreduce / 20% reduce_scatter / 20% allgather, P on [4, 4096], "
@@ -957,6 +967,7 @@ def main():
     ap.add_argument("--picker-seed", type=int, default=11)
     ap.add_argument("--picker-budget", type=float, default=900.0, help="seconds of measurement at most")
     ap.add_argument("--picker-steps", type=int, default=8000)
+    ap.add_argument("--picker-ensemble", type=int, default=5, help="models trained with different seeds, averaged")
     ap.add_argument("--picker-data", default=None,
                     help="measured picker_dataset.npz files to train on (comma-separated; --picker-n 0 to measure none)")
     ap.add_argument("--picker-repeat", type=int, default=150, help="held-out calls re-timed for the noise ceiling")

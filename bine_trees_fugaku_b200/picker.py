@@ -353,9 +353,12 @@ def train(X, Y, M, steps=3000, batch=256, lr=1e-3, seed=0, log=None, val=None, c
 
 
 def predict(mlp, X):
-    """Model outputs [n, OUT_DIM] (standardised log2 time, log2 link bytes)."""
+    """Model outputs [n, OUT_DIM] (standardised log2 time, log2 link bytes);
+    for a list of models (an ensemble), the mean of their outputs."""
     import torch
 
+    if isinstance(mlp, (list, tuple)):
+        return np.mean([predict(m, X) for m in mlp], axis=0)
     n = X.shape[0]
     pad = (-n) % 16
     Xp = np.concatenate([X, np.zeros((pad, IN_DIM), np.float32)]) if pad else X
@@ -416,27 +419,30 @@ def evaluate(pred, T, Lb, valid, configs, shortlist=3):
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "picker_weights.npz")
 
 
-def save(path, mlp, stats, meta):
-    """Saves the weights as the bf16 values the forward pass uses (the
-    master copies are fp32; forward rounds them to bf16)."""
-    meta = dict(meta, feature_version=FEATURE_VERSION)
-    p = mlp.get_params()
+def save(path, mlps, stats, meta):
+    """Saves the weights of one model or of an ensemble (a list) as the
+    bf16 values the forward pass uses (the master copies are fp32; forward
+    rounds them to bf16), one row per model."""
+    mlps = mlps if isinstance(mlps, (list, tuple)) else [mlps]
+    meta = dict(meta, feature_version=FEATURE_VERSION, models=len(mlps))
+    p = np.stack([m.get_params() for m in mlps])
     bits = (p.view(np.uint32) + 0x7FFF + ((p.view(np.uint32) >> 16) & 1)) >> 16  # round to nearest even
     np.savez_compressed(path, params_bf16=bits.astype(np.uint16), stats=json.dumps(stats),
                         meta=json.dumps(meta), arms=json.dumps(ARMS), dims=np.array([IN_DIM, 256, OUT_DIM]))
 
 
 def load_params(path):
-    """(params as float32, dims, stats, meta) of a saved picker."""
+    """(params as float32 [models, n], dims, stats, meta, arms) of a saved
+    picker."""
     z = np.load(path)
     p = (z["params_bf16"].astype(np.uint32) << 16).view(np.float32)
-    return p, tuple(int(v) for v in z["dims"]), json.loads(str(z["stats"])), json.loads(str(z["meta"])), \
-        json.loads(str(z["arms"]))
+    return np.atleast_2d(p), tuple(int(v) for v in z["dims"]), json.loads(str(z["stats"])), \
+        json.loads(str(z["meta"])), json.loads(str(z["arms"]))
 
 
 class Picker:
     """Runtime picker.  With trained weights it ranks the arms by predicted
-    time (bine_mlp forward on the GPU) and takes the first one the planner
+    time (bine_mlp forward on the GPU, averaged over the ensemble) and takes the first one the planner
     proves correct for the call; without weights it takes the fixed rule,
     then the latency-optimal tree (allreduce) or the block-by-block
     allgather when the planner refuses the rule's arm.  Picks are cached
@@ -452,8 +458,11 @@ class Picker:
             if [tuple(a) for a in arms] != ARMS or dims != (IN_DIM, 256, OUT_DIM) or \
                     meta.get("feature_version") != FEATURE_VERSION:
                 raise ValueError(f"{path}: arm space, features or model shape differ from this build")
-            self.mlp = bine.MLP(dims[0], dims[1], dims[2], 16, seed=0)
-            self.mlp.set_params(p)
+            self.mlp = []
+            for row in p:  # an ensemble: predictions are averaged
+                m = bine.MLP(dims[0], dims[1], dims[2], 16, seed=0)
+                m.set_params(row)
+                self.mlp.append(m)
 
     def ranking(self, coll, P, count, es, dims=None):
         """Candidate arm indices, best first."""

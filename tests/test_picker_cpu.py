@@ -140,6 +140,9 @@ def test_saved_weights_are_the_bf16_forward_values(tmp_path):
     path = tmp_path / "w.npz"
     pk.save(str(path), Fake(), {"t_mean": 0.0}, {"calls": 0})
     p, dims, st, meta, arms = pk.load_params(str(path))
-    assert list(p) == [1.0, 1.0, 1.0078125, -2.5, 3.140625]
+    assert p.shape == (1, 5) and list(p[0]) == [1.0, 1.0, 1.0078125, -2.5, 3.140625]
+    pk.save(str(path), [Fake(), Fake()], {"t_mean": 0.0}, {"calls": 0})
+    p, _, _, meta, _ = pk.load_params(str(path))
+    assert p.shape == (2, 5) and meta["models"] == 2
     assert dims == (pk.IN_DIM, 256, pk.OUT_DIM) and [tuple(a) for a in arms] == pk.ARMS
     assert json.dumps(st) and meta["calls"] == 0

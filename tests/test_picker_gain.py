@@ -34,8 +34,7 @@ def load():
 
 def cpu_predict(X):
     p, dims, _, _, _ = pk.load_params(pk.DEFAULT_WEIGHTS)
-    pres, _ = mlp_ref.forward(p, bine.mlp_layout(*dims), X)
-    return pres[-1]
+    return np.mean([mlp_ref.forward(row, bine.mlp_layout(*dims), X)[0][-1] for row in p], axis=0)
 
 
 def check_gain(ev):
@@ -44,7 +43,7 @@ def check_gain(ev):
     # than the fixed rule on average; the model's three best arms, timed,
     # hold an arm within 5 % of the optimum on >= 95 % of the calls.
     assert ev["held_out_calls"] >= 900
-    assert ev["pick_within_5pct_of_optimum"] >= 0.87
+    assert ev["pick_within_5pct_of_optimum"] >= 0.89
     assert ev["pick_within_5pct_of_optimum"] >= ev["fixed_rule_within_5pct_of_optimum"] + 0.4
     assert ev["pick_time_over_optimum_geomean"] <= 1.03
     assert ev["shortlist3_within_5pct_of_optimum"] >= 0.95
