@@ -502,6 +502,7 @@ def run_batch_suite(args):
 SWEEP_COLLS = ["allreduce", "reduce_scatter", "allgather", "bcast", "alltoall"]
 SWEEP_P = [16, 64, 96, 256, 384, 1024]
 SWEEP_BYTES = [32 * 4 ** k for k in range(11)] + [64 << 20]
+SWEEP_ENGINES = ("fused", "steps", "pipelined")
 
 
 def sweep_algo_bytes(coll, P, count, es):
@@ -556,7 +557,8 @@ def run_sweep_suite(args):
     contribution 32 B..16 MiB in powers of 4 and 64 MiB, float32 N(0,1) and
     int64 U[-2^40, 2^40].  Each point is checked (sweep_check) and timed on
     the device: FUSED engine in the reference float order where the
-    reference has one (else FAST), and the STEPS engine up to P=384.
+    reference has one (else FAST), and the STEPS and PIPELINED engines up
+    to P=384.
     Points whose device working set exceeds 80 % of free HBM are skipped and
     listed.  One JSON line per point goes to --out/sweep.jsonl; a summary
     line to stdout."""
@@ -600,7 +602,7 @@ def run_sweep_suite(args):
 
         for P in SWEEP_P:
             comms = {}
-            for engine in ("fused", "steps"):
+            for engine in SWEEP_ENGINES:
                 cm = bine.Comm(P)
                 cm.set_engine(engine)
                 cm.set_stream(stream)
@@ -625,8 +627,8 @@ def run_sweep_suite(args):
                         recv = torch.zeros((P, re), dtype=tdt, device="cuda")
                         if coll == "bcast":
                             recv[0] = send[0]
-                        for engine in ("fused", "steps"):
-                            if engine == "steps" and P > 384:
+                        for engine in SWEEP_ENGINES:
+                            if engine != "fused" and P > 384:
                                 continue
                             comm = comms[engine]
                             order = "reference"
@@ -635,7 +637,7 @@ def run_sweep_suite(args):
                                 try:
                                     t_us = time_call(comm, coll, send, recv, count, code)
                                 except bine.Unsupported:
-                                    if engine == "steps" or dname != "float32":
+                                    if engine != "fused" or dname != "float32":
                                         raise
                                     order = "fast"  # the reference has no float order to keep here
                                     comm.set_float_order("fast")
@@ -691,7 +693,19 @@ def run_sweep_suite(args):
         k = (r["coll"], r["engine"])
         if k not in best or r["algo_gbs"] > best[k]["algo_gbs"]:
             best[k] = r
+    import numpy as np
+
+    # The two schedule-faithful engines point by point: geometric mean of
+    # the STEPS time over the PIPELINED time, by per-rank message size.
+    us = {(r["coll"], r["P"], r["bytes_per_rank"], r["dtype"], r["engine"]): r["us"] for r in timed}
+    ratio = {}
+    for (coll, P, nb, dt, eng), t in us.items():
+        if eng == "steps" and (coll, P, nb, dt, "pipelined") in us:
+            band = "below 64 KiB" if nb < 65536 else ("64 KiB to 2 MiB" if nb < 2 << 20 else "2 MiB and up")
+            ratio.setdefault(band, []).append(t / us[(coll, P, nb, dt, "pipelined")])
     line = {"suite": "sweep", "points_timed": len(timed), "points_incorrect": len(bad),
+            "steps_over_pipelined_time_geomean": {k: round(float(np.exp(np.mean(np.log(v)))), 3)
+                                                  for k, v in sorted(ratio.items())},
             "reference_points": len([r for r in refs if "speedup" in r]),
             "speedup_over_reference_range": [round(min(r["speedup"] for r in refs if "speedup" in r), 1),
                                              round(max(r["speedup"] for r in refs if "speedup" in r), 1)]
@@ -953,7 +967,7 @@ def main():
     ap.add_argument("--P", type=int, default=256)
     ap.add_argument("--count", type=int, default=1 << 20)
     ap.add_argument("--dtype", default="int32", choices=["int32", "float"])
-    ap.add_argument("--engine", default="fused", choices=["fused", "steps"])
+    ap.add_argument("--engine", default="fused", choices=["fused", "steps", "pipelined"])
     ap.add_argument("--order", default="reference", choices=["reference", "fast"])
     ap.add_argument("--host-window", type=int, default=32 << 20,
                     help="column-window bytes of the host-buffer pipeline (e2e leg)")

@@ -21,7 +21,7 @@ from .build import LIB_PATH
 INT32, INT64, FLOAT, DOUBLE, CHAR = 0, 1, 2, 3, 4
 SUM = 0
 SUCCESS, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_INTERNAL = range(7)
-ENGINE_FUSED, ENGINE_STEPS = 0, 1
+ENGINE_FUSED, ENGINE_STEPS, ENGINE_PIPELINED = 0, 1, 2
 ORDER_REFERENCE, ORDER_FAST = 0, 1
 FAMILY = {"BINE": 1, "RECDOUB": 2, "BRUCK": 3}
 DISTANCE = {None: -1, "INCREASING": 0, "DECREASING": 1}
@@ -127,6 +127,8 @@ def lib():
         "bine_link_bytes": [vp, i, ctypes.c_long, i, i, vp],
         "bine_plan_moves": [vp, i, ctypes.c_long, i, i64p, i64p, sz, ctypes.POINTER(sz)],
         "bine_plan_messages": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz)],
+        "bine_plan_flow": [vp, i, ctypes.c_long, i, i, i, i64p, sz, ctypes.POINTER(sz), ctypes.POINTER(ctypes.c_int32),
+                           sz, ctypes.POINTER(sz), ctypes.POINTER(ctypes.c_int32), sz, ctypes.POINTER(sz)],
         "bine_plan_trees": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz)],
         "bine_link_bytes_host": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(ctypes.c_uint64), sz],
         "bine_mlp_create": [i, i, i, i, ctypes.c_ulonglong, ctypes.POINTER(vp)],
@@ -234,7 +236,8 @@ class Comm:
                                        DISTANCE[distance]))
 
     def set_engine(self, engine):
-        check(lib().bine_comm_set_engine(self._h, {"fused": ENGINE_FUSED, "steps": ENGINE_STEPS}.get(engine, engine)))
+        check(lib().bine_comm_set_engine(self._h, {"fused": ENGINE_FUSED, "steps": ENGINE_STEPS,
+                                                             "pipelined": ENGINE_PIPELINED}.get(engine, engine)))
 
     def set_segment(self, segment_bytes):
         check(lib().bine_comm_set_segment(self._h, segment_bytes))
@@ -337,6 +340,23 @@ class Comm:
                                     mv.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                                     sz.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n.value, ctypes.byref(n)))
         return mv[: n.value], sz[: n.value] // 2, sz[: n.value] % 2
+
+    def plan_flow(self, coll, count, root=0, elem_size=4, target_items=592):
+        """Dataflow form of the schedule as the PIPELINED engine runs it:
+        (pieces [n, 3] = move, start, n; items [n, 5] = piece begin/end,
+        dependency begin/end, level; deps: item index or -(level + 1))."""
+        npc, nit, ndp = ctypes.c_size_t(0), ctypes.c_size_t(0), ctypes.c_size_t(0)
+        check(lib().bine_plan_flow(self._h, COLL_ID[coll], count, root, elem_size, target_items, None, 0,
+                                   ctypes.byref(npc), None, 0, ctypes.byref(nit), None, 0, ctypes.byref(ndp)))
+        pieces = np.zeros((max(1, npc.value), 3), np.int64)
+        items = np.zeros((max(1, nit.value), 5), np.int32)
+        deps = np.zeros(max(1, ndp.value), np.int32)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        check(lib().bine_plan_flow(self._h, COLL_ID[coll], count, root, elem_size, target_items,
+                                   pieces.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), npc.value, ctypes.byref(npc),
+                                   items.ctypes.data_as(i32p), nit.value, ctypes.byref(nit),
+                                   deps.ctypes.data_as(i32p), ndp.value, ctypes.byref(ndp)))
+        return pieces[: npc.value], items[: nit.value], deps[: ndp.value]
 
     def plan_messages(self, coll, count, root=0):
         n = ctypes.c_size_t(0)

@@ -21,6 +21,9 @@
 //   k_steps      the reference's schedule executed level by level in one
 //                cooperative launch, with a bounded grid-wide barrier between
 //                levels that reports a timeout instead of hanging.
+//   k_flow       the same schedule as a dataflow of segments: each starts
+//                when the segments it reads and overwrites are done (bounded
+//                waits on per-segment completion flags), so steps overlap.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -748,6 +751,180 @@ __global__ void __launch_bounds__(kThreads) k_steps(StepBufs B, const StepMove* 
             run_chunk<T>(B, moves[ch.move], ch);
         }
         if (l + 1 < nlevels && !grid_barrier(bar, status, timeout_ns, expected)) return;
+    }
+}
+
+// ------------------------------------------------- pipelined step engine
+// The schedule as a dataflow of items (packed segments of moves, one level
+// each; built on the host by build_flow).  Blocks take items in index order
+// from a global counter and run each one once the items it depends on are
+// done, so a segment moves on to the next step as soon as the segments it
+// reads and overwrites are ready: steps overlap, ports proceed
+// independently, and no block waits for the slowest block of a level.
+//
+// Dependencies only point to earlier items, which were handed to running
+// blocks before, so the waits always end; they are bounded nevertheless.
+// State (zero-initialised once): done[item] holds the epoch of the call that
+// completed it; ctl[0] is the next item, ctl[1] the blocks finished, ctl[2]
+// the epoch of the last completed call, ctl[3 + l] the items of level l
+// done.  The last block to finish resets the counters and advances the
+// epoch, so consecutive launches need no memset.
+struct FlowItem {
+    int32_t pbeg, pend, dbeg, dend, level, pad;
+};
+constexpr int kFlowPieces = 256;  // pieces per item, at most one per thread
+constexpr int kFlowUnroll = 4;    // 16-byte units in flight per thread
+
+__device__ __forceinline__ bool flow_wait(int dep, const unsigned* done, const unsigned* ctl,
+                                          const int* level_items, unsigned target, unsigned extra, int* status,
+                                          unsigned long long timeout_ns) {
+    const bool item = dep >= 0;
+    const unsigned* p = item ? &done[dep] : &ctl[3 + (-dep - 1)];
+    const unsigned need = item ? target + extra : (unsigned)level_items[-dep - 1] + extra;
+    if (item ? ld_acquire(p) == need : ld_acquire(p) >= need) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (unsigned long long iters = 0;; iters++) {
+        const unsigned v = ld_acquire(p);
+        if (item ? v == need : v >= need) return true;
+        if (iters > (1ull << 40) || globaltimer_ns() - t0 > timeout_ns || *(volatile int*)status != kStepOk) {
+            atomicCAS(status, kStepOk, kStepTimeout);
+            return false;
+        }
+        __nanosleep(32);
+    }
+}
+
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Completion is a release store after the block barrier (release is
+// cumulative over the block's writes), read with acquire loads.
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove* __restrict__ moves,
+                                                      const StepChunk* __restrict__ pieces,
+                                                      const FlowItem* __restrict__ items, int nitems,
+                                                      const int* __restrict__ deps,
+                                                      const int* __restrict__ level_items, int nlevels,
+                                                      unsigned* done, unsigned* ctl, int* status,
+                                                      unsigned long long timeout_ns, unsigned extra) {
+    __shared__ long long s_pref[kFlowPieces + 1];  // first unit of each piece
+    __shared__ char* s_d[kFlowPieces];
+    __shared__ const char* s_a[kFlowPieces];
+    __shared__ const char* s_b[kFlowPieces];
+    __shared__ unsigned char s_kind[kFlowPieces];  // bit 0: add, bit 1: 16-byte units
+    __shared__ long long s_warp[kThreads / 32];
+    __shared__ int s_item, s_ok;
+    __shared__ unsigned s_target;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        const unsigned t = ld_acquire(&ctl[2]) + 1u;
+        s_target = t == 0 ? 1u : t;  // 0 is the initial value of done[]
+    }
+    __syncthreads();
+    const unsigned target = s_target;
+    constexpr long long es = sizeof(T);
+    for (;;) {
+        if (tid == 0) s_item = *(volatile int*)status == kStepOk ? (int)atomicAdd(&ctl[0], 1u) : nitems;
+        __syncthreads();
+        const int i = s_item;
+        if (i >= nitems) break;
+        const FlowItem it = items[i];
+        // Piece table (addresses, unit kind and count; tables only, no data
+        // rows) before the dependency wait, so that it is off the critical
+        // path; then a block scan of the unit counts.
+        const int np = it.pend - it.pbeg;
+        long long units = 0;
+        if (tid < np) {
+            const StepChunk ch = pieces[it.pbeg + tid];
+            const StepMove m = moves[ch.move];
+            char* d = B.base[m.dst_buf] + (long long)m.dst_rank * B.stride[m.dst_buf] + (m.dst_off + ch.start) * es;
+            const char* a = B.base[m.a_buf] + (long long)m.a_rank * B.stride[m.a_buf] + (m.a_off + ch.start) * es;
+            const char* b = B.base[m.b_buf] + (long long)m.b_rank * B.stride[m.b_buf] + (m.b_off + ch.start) * es;
+            const long long bytes = ch.n * es;
+            const bool vec = (((uintptr_t)d | (uintptr_t)a | (uintptr_t)(m.add ? b : a)) & 15) == 0 && (bytes & 15) == 0;
+            units = vec ? bytes / 16 : ch.n;
+            s_d[tid] = d;
+            s_a[tid] = a;
+            s_b[tid] = b;
+            s_kind[tid] = (unsigned char)((m.add ? 1 : 0) | (vec ? 2 : 0));
+        }
+        if (warp == 0) {
+            bool ok = true;
+            for (int d = it.dbeg + lane; d < it.dend && ok; d += 32)
+                ok = flow_wait(deps[d], done, ctl, level_items, target, extra, status, timeout_ns);
+            ok = __all_sync(0xffffffffu, ok);
+            if (lane == 0) s_ok = ok;
+        }
+        long long inc = units;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        long long before = 0;
+        for (int w = 0; w < warp; w++) before += s_warp[w];
+        s_pref[tid + 1] = before + inc;
+        if (tid == 0) s_pref[0] = 0;
+        __syncthreads();
+        if (!s_ok) break;  // a wait expired; the status is recorded
+        const long long total = s_pref[np];
+        int cur = 0;
+        for (long long u0 = tid; u0 < total; u0 += (long long)kFlowUnroll * kThreads) {
+            uint4 va[kFlowUnroll], vb[kFlowUnroll];
+            char* dp[kFlowUnroll];
+            int kind[kFlowUnroll];
+#pragma unroll
+            for (int k = 0; k < kFlowUnroll; k++) {
+                const long long u = u0 + (long long)k * kThreads;
+                kind[k] = -1;
+                if (u < total) {
+                    if (!(u >= s_pref[cur] && u < s_pref[cur + 1])) {
+                        int lo = 0, hi = np - 1;  // last piece starting at or before u
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (s_pref[mid] <= u) lo = mid; else hi = mid - 1;
+                        }
+                        cur = lo;
+                    }
+                    const long long r = u - s_pref[cur];
+                    const int kd = s_kind[cur];
+                    // Plain (coherent) loads: other blocks wrote these rows
+                    // during this launch.
+                    if (kd & 2) {
+                        kind[k] = kd;
+                        dp[k] = s_d[cur] + r * 16;
+                        va[k] = ld_plain(s_a[cur] + r * 16);
+                        if (kd & 1) vb[k] = ld_plain(s_b[cur] + r * 16);
+                    } else {  // element units (unaligned pieces): done at once
+                        T v = *((volatile const T*)s_a[cur] + r);
+                        if (kd & 1) v = add_exact<T>(v, *((volatile const T*)s_b[cur] + r));
+                        *((T*)s_d[cur] + r) = v;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kFlowUnroll; k++)
+                if (kind[k] >= 0) *(uint4*)dp[k] = (kind[k] & 1) ? vadd<T>(va[k], vb[k]) : va[k];
+        }
+        __syncthreads();
+        if (tid == 0) {
+            st_release(&done[i], target);
+            red_release_add(&ctl[3 + it.level], 1u);
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&ctl[1], 1u) == gridDim.x - 1) {
+            ctl[0] = 0;
+            ctl[1] = 0;
+            for (int l = 0; l < nlevels; l++) ctl[3 + l] = 0;
+            __threadfence();
+            st_release(&ctl[2], target);
+        }
     }
 }
 

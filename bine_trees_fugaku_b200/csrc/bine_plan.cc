@@ -1852,3 +1852,150 @@ bool split_trees(const TreePlan& tp, int K, SplitTrees* out, std::string* err) {
 }
 
 }  // namespace bine
+
+// ------------------------------------------------------------- dataflow plan
+namespace bine {
+namespace {
+
+// Element ranges of one row: start -> span.  Spans cover what some item has
+// touched; untouched gaps have no writer and no readers.
+struct FlowSpan {
+    int64_t end;
+    int32_t writer;                // last item that wrote the span, -1: none
+    std::vector<int32_t> readers;  // items that read it since (ascending)
+};
+using FlowRow = std::map<int64_t, FlowSpan>;
+
+// Splits the span containing x (if x falls strictly inside one) at x.
+void flow_split(FlowRow& row, int64_t x) {
+    auto it = row.upper_bound(x);
+    if (it == row.begin()) return;
+    --it;
+    if (it->first < x && x < it->second.end) {
+        FlowSpan right = it->second;
+        it->second.end = x;
+        row.emplace(x, std::move(right));
+    }
+}
+
+// Makes [s, e) a sequence of spans (gaps filled with untouched spans) and
+// calls f on each.
+template <typename F>
+void flow_cover(FlowRow& row, int64_t s, int64_t e, F f) {
+    flow_split(row, s);
+    flow_split(row, e);
+    int64_t pos = s;
+    auto it = row.lower_bound(s);
+    while (pos < e) {
+        if (it == row.end() || it->first > pos) {
+            const int64_t gap_end = it == row.end() ? e : std::min(e, it->first);
+            it = row.emplace_hint(it, pos, FlowSpan{gap_end, -1, {}});
+        }
+        f(it->second);
+        pos = it->second.end;
+        ++it;
+    }
+}
+
+}  // namespace
+
+void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
+                int target_items, FlowPlan* out) {
+    *out = FlowPlan();
+    const bool auto_pieces = piece_elems <= 0;
+    target_items = std::max(1, target_items);
+    min_item_elems = std::max<int64_t>(1, min_item_elems);
+    max_item_elems = std::max(min_item_elems, max_item_elems);
+    // Pieces and items, level by level.
+    std::vector<const Move*> move_of;  // level-order move index -> move
+    for (size_t l = 0; l < s.levels.size(); l++) {
+        int64_t level_elems = 0;
+        for (const Move& m : s.levels[l]) level_elems += m.n;
+        int64_t item_elems = std::max(min_item_elems, (level_elems + target_items - 1) / target_items);
+        if (auto_pieces) {
+            // Whole multiples of min_item_elems, so that pieces cut from a
+            // move start on the same alignment as the move.
+            item_elems = std::min(max_item_elems, (item_elems + min_item_elems - 1) / min_item_elems * min_item_elems);
+            piece_elems = item_elems;
+        } else {
+            item_elems = std::min(item_elems, piece_elems);
+        }
+        int32_t nitems = 0;
+        int64_t cur = 0;  // elements in the open item
+        for (const Move& m : s.levels[l]) {
+            const int32_t mi = (int32_t)move_of.size();
+            move_of.push_back(&m);
+            for (int64_t st = 0; st < m.n; st += piece_elems) {
+                const int64_t n = std::min(piece_elems, m.n - st);
+                if (nitems == 0 || cur + n > item_elems ||
+                    out->items.back().pend - out->items.back().pbeg >= kFlowMaxPieces) {
+                    const int32_t p = (int32_t)out->pieces.size();
+                    out->items.push_back(FlowItem{p, p, 0, 0, (int32_t)l, 0});
+                    nitems++;
+                    cur = 0;
+                }
+                out->pieces.push_back(FlowPiece{mi, 0, st, n});
+                out->items.back().pend++;
+                cur += n;
+            }
+        }
+        out->level_items.push_back(nitems);
+    }
+    // Dependencies over rows (buffer, rank); send and receive rows share one
+    // row space.
+    auto row_id = [&](const Region& r) { return (r.buf == kBufTmp ? P : 0) + r.rank; };
+    std::vector<FlowRow> rows(2 * (size_t)P);
+    std::vector<int32_t> cand;
+    for (int32_t i = 0; i < (int32_t)out->items.size(); i++) {
+        FlowItem& it = out->items[i];
+        cand.clear();
+        // Reads first: read after write on the last writers; the item
+        // becomes a reader.
+        for (int32_t p = it.pbeg; p < it.pend; p++) {
+            const FlowPiece& pc = out->pieces[p];
+            const Move& m = *move_of[pc.move];
+            for (int k = 0; k < 1 + m.add; k++) {
+                const Region& r = k ? m.b : m.a;
+                flow_cover(rows[row_id(r)], r.off + pc.start, r.off + pc.start + pc.n, [&](FlowSpan& sp) {
+                    if (sp.writer >= 0) cand.push_back(sp.writer);
+                    if (sp.readers.empty() || sp.readers.back() != i) sp.readers.push_back(i);
+                });
+            }
+        }
+        // Then writes: write after write on the last writer, write after
+        // read on the readers since; the item becomes the writer.
+        for (int32_t p = it.pbeg; p < it.pend; p++) {
+            const FlowPiece& pc = out->pieces[p];
+            const Move& m = *move_of[pc.move];
+            FlowRow& row = rows[row_id(m.dst)];
+            const int64_t s0 = m.dst.off + pc.start, s1 = s0 + pc.n;
+            flow_cover(row, s0, s1, [&](FlowSpan& sp) {
+                if (sp.writer >= 0) cand.push_back(sp.writer);
+                cand.insert(cand.end(), sp.readers.begin(), sp.readers.end());
+            });
+            row.erase(row.lower_bound(s0), row.lower_bound(s1));
+            row.emplace(s0, FlowSpan{s1, i, {}});
+        }
+        // Earlier levels only, one entry per item, and a level entry where
+        // one level would contribute more than kFlowLevelDep items.
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        it.dbeg = (int32_t)out->deps.size();
+        size_t j = 0;
+        while (j < cand.size()) {
+            const int32_t lv = out->items[cand[j]].level;
+            size_t k = j;
+            while (k < cand.size() && out->items[cand[k]].level == lv) k++;
+            if (lv < it.level) {
+                if (k - j > (size_t)kFlowLevelDep)
+                    out->deps.push_back(-(lv + 1));
+                else
+                    out->deps.insert(out->deps.end(), cand.begin() + j, cand.begin() + k);
+            }
+            j = k;
+        }
+        it.dend = (int32_t)out->deps.size();
+    }
+}
+
+}  // namespace bine

@@ -164,6 +164,46 @@ class Planner {
     Torus t_;
 };
 
+// Dataflow form of a schedule, for the pipelined engine.  Every move is cut
+// into pieces of at most `piece_elems` elements; consecutive pieces of one
+// level are packed into items (at most kFlowMaxPieces pieces and about
+// level elements / `target_items` elements each, never below
+// `min_item_elems` unless the level is smaller).  With piece_elems <= 0 the
+// pieces take the item size of their level, rounded up to a multiple of
+// `min_item_elems` and capped at `max_item_elems`.  Each item lists the
+// earlier items it must wait for over every (buffer, rank) row: the last
+// writer of what it reads (read after write) and of what it writes (write
+// after write), and every reader since that writer of what it writes (write
+// after read).  A dependency is an item index >= 0, or -(l + 1) for "every
+// item of level l", used where one level would contribute more than
+// kFlowLevelDep items.  Items are in level order and every dependency is on
+// an earlier level, so running items in index order, each after its
+// dependencies, is deadlock free and computes what level-by-level execution
+// computes.
+constexpr int kFlowMaxPieces = 256;
+constexpr int kFlowLevelDep = 8;
+
+struct FlowPiece {  // elements [start, start + n) of move `move` (level-order index)
+    int32_t move, pad;
+    int64_t start, n;
+};
+struct FlowItem {  // pieces [pbeg, pend), dependencies [dbeg, dend)
+    int32_t pbeg, pend, dbeg, dend, level, pad;
+};
+struct FlowPlan {
+    std::vector<FlowPiece> pieces;
+    std::vector<FlowItem> items;
+    std::vector<int32_t> deps;
+    std::vector<int32_t> level_items;  // items per level
+};
+
+// The send and receive rows of a rank are tracked as one row (an in-place
+// call aliases them).  Moves of one level never wait for each other: as in
+// level-by-level execution, the planner emits levels whose moves are
+// independent.
+void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
+                int target_items, FlowPlan* out);
+
 // Per-link byte counts of a message list on the torus: 2 * ndims directed
 // links per node, index (node * ndims + d) * 2 + (dir > 0 ? 0 : 1).
 // Routes are dimension-ordered and minimal per dimension (+ on ties).

@@ -85,8 +85,14 @@ enum { BINE_DISTANCE_INCREASING = 0, BINE_DISTANCE_DECREASING = 1, BINE_DISTANCE
  *     exact addition tree per element in registers;
  *   STEPS: one persistent kernel that executes the reference's schedule step
  *     by step (the message pattern of the MPI layer, as device loads and
- *     stores), with a bounded grid-wide barrier between steps. */
-enum { BINE_ENGINE_FUSED = 0, BINE_ENGINE_STEPS = 1 };
+ *     stores), with a bounded grid-wide barrier between steps;
+ *   PIPELINED: the same schedule and moves as STEPS, cut into segments that
+ *     each start as soon as the segments they read and overwrite are done,
+ *     with no barrier between steps: steps overlap segment by segment and
+ *     ports proceed independently (the device analogue of the uTofu layer's
+ *     per-port threads and segmented transfers, lib/libbine_common.cc:1741-1879).
+ *     Results equal the STEPS engine's, float32 included. */
+enum { BINE_ENGINE_FUSED = 0, BINE_ENGINE_STEPS = 1, BINE_ENGINE_PIPELINED = 2 };
 
 /* Floating-point summation order for the FUSED engine.
  *   REFERENCE (default): bit-identical to the reference's per-step order;
@@ -118,10 +124,11 @@ int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int fami
 
 int bine_comm_set_engine(bine_comm_t comm, int engine);
 
-/* LIBBINE_SEGMENT_SIZE analogue for the STEPS engine: bytes of each unit of
- * work a block takes (0: 32 KiB).  Small segments spread small messages
- * over more blocks; large ones cut per-chunk overhead.  Results do not
- * depend on it. */
+/* LIBBINE_SEGMENT_SIZE analogue for the STEPS and PIPELINED engines: bytes
+ * of each unit of work a block takes (0: 32 KiB).  Small segments spread
+ * small messages over more blocks (and, PIPELINED, let a step start on a
+ * message's first segment before its last one is ready); large ones cut
+ * per-segment overhead.  Results do not depend on it. */
 int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes);
 int bine_comm_set_float_order(bine_comm_t comm, int order);
 
@@ -204,20 +211,23 @@ int bine_allreduce_noalloc(const void *sendbuf, void *recvbuf, int count, bine_d
                            bine_comm_t comm);
 
 /* Waits for the communicator's stream and reports device-side errors
- * (BINE_ERR_TIMEOUT when a bounded barrier of the STEPS engine expired). */
+ * (BINE_ERR_TIMEOUT when a bounded barrier of the STEPS engine, or a
+ * bounded segment wait of the PIPELINED engine, expired). */
 int bine_comm_synchronize(bine_comm_t comm);
 
 const char *bine_last_error_string(void);
 
-/* Bound of every device-side wait of the STEPS engine (grid barriers between
- * steps), in milliseconds; default 5000.  A wait that expires makes the
+/* Bound of every device-side wait of the STEPS and PIPELINED engines (grid
+ * barriers between steps, segment waits), in milliseconds; default 5000.  A wait that expires makes the
  * kernel record the timeout and return; bine_comm_synchronize() then
  * reports BINE_ERR_TIMEOUT and the context stays usable. */
 int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms);
 
 /* Fault injection for tests of the timeout path: makes every grid barrier of
- * the STEPS engine wait for `extra` arrivals that never come, so the bounded
- * wait expires (0 restores normal operation).  Nothing faults or hangs. */
+ * the STEPS engine wait for `extra` arrivals that never come, and every
+ * segment wait of the PIPELINED engine for a completion that never comes,
+ * so the bounded wait expires (0 restores normal operation).  Nothing
+ * faults or hangs. */
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
 
 /* Lanes that cooperate on one output vector in the exact-order float
@@ -326,6 +336,16 @@ int bine_plan_moves(bine_comm_t comm, bine_coll_t coll, long count, int root, in
                     size_t cap, size_t *n_moves);
 
 /* The reference's messages of the call: (level, src, dst, elements). */
+/* Dataflow form of a call's schedule as the PIPELINED engine runs it, for
+ * tests and tools.  pieces[n][3]: (move index in bine_plan_moves order,
+ * first element, elements); items[n][5]: (first piece, end piece, first
+ * dependency, end dependency, level); deps[n]: an item index, or -(l + 1)
+ * for every item of level l.  `elem_size` and `target_items` stand for the
+ * datatype and for the engine's four items per SM per level. */
+int bine_plan_flow(bine_comm_t comm, bine_coll_t coll, long count, int root, int elem_size, int target_items,
+                   int64_t *pieces, size_t piece_cap, size_t *n_pieces, int32_t *items, size_t item_cap,
+                   size_t *n_items, int32_t *deps, size_t dep_cap, size_t *n_deps);
+
 int bine_plan_messages(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t *msgs, size_t cap,
                        size_t *n_msgs);
 

@@ -1,7 +1,8 @@
 """GPU parity of the engine, through the C ABI, against the reference.
 
 * Every golden case (outputs of the reference library itself) is run on the
-  FUSED and on the STEPS engine and compared bit for bit, float32 included.
+  FUSED, STEPS and PIPELINED engines and compared bit for bit, float32
+  included.
 * Larger cases are compared with the oracle (the C++ restatement).
 * Full-size properties (P = 256, 4 MiB per rank) use exact integer sums and
   the FP64 tolerance of the reordered float path.
@@ -51,13 +52,16 @@ def case_id(c):
             f"-r{c.get('root', 0)}-{c.get('family', 'BINE')}")
 
 
-@pytest.mark.parametrize("engine", ["fused", "steps"])
+@pytest.mark.parametrize("engine", ["fused", "steps", "pipelined", "pipelined-seg256"])
 @pytest.mark.parametrize("case", CASES, ids=case_id)
 def test_engine_matches_reference(case, engine):
     x = case_input(case)
     root = case.get("root", 0)
+    segment = 256 if engine.endswith("seg256") else 0  # many small segments, level dependencies
+    engine = engine.split("-")[0]
     comm = make_comm(case["P"], case["coll"], case["variant"], case.get("dims"), case.get("ports", 1),
                      case.get("family", "BINE"), case.get("distance"), engine)
+    comm.set_segment(segment)
     rr = receiving_ranks(case["coll"], case["P"], root)
     reduction = case["coll"] in ("allreduce", "reduce_scatter", "reduce")
     right = reference_is_right(case, x)
@@ -67,7 +71,7 @@ def test_engine_matches_reference(case, engine):
         # Only cases where the reference fails or returns wrong data may be
         # refused, and only by the engine that follows the reference's
         # schedule or by the exact float order.
-        assert engine == "steps" or (reduction and case["dtype"] == "float")
+        assert engine in ("steps", "pipelined") or (reduction and case["dtype"] == "float")
         assert not right
         return
     if right:
@@ -98,7 +102,7 @@ def reference_is_right(case, x):
     return bool(np.array_equal(case["out"][rr], exp[rr]))
 
 
-@pytest.mark.parametrize("engine", ["fused", "steps"])
+@pytest.mark.parametrize("engine", ["fused", "steps", "pipelined"])
 @pytest.mark.parametrize("coll,variant,P,count,dims,ports", [
     ("allreduce", "B", 64, 64 * 1000 + 13, None, 1),
     ("allreduce", "B", 96, 96 * 512, None, 1),
@@ -181,13 +185,14 @@ def test_full_size_int32_allreduce_is_exact():
     assert torch.equal(recv, expect.expand(P, count))
 
 
+@pytest.mark.parametrize("engine", ["steps", "pipelined"])
 @pytest.mark.parametrize("P,count", [(256, 1 << 18), (1024, 1 << 14)])
-def test_full_size_int32_allreduce_steps_engine(P, count):
+def test_full_size_int32_allreduce_steps_engine(P, count, engine):
     g = torch.Generator(device="cuda")
     g.manual_seed(2)
     send = torch.randint(-1000, 1001, (P, count), dtype=torch.int32, device="cuda", generator=g)
     recv = torch.empty_like(send)
-    comm = make_comm(P, "allreduce", "B", engine="steps")
+    comm = make_comm(P, "allreduce", "B", engine=engine)
     comm.allreduce(send, recv, count, bine.INT32)
     comm.synchronize()
     assert torch.equal(recv, send.sum(0, dtype=torch.int64).to(torch.int32).expand(P, count))
@@ -249,13 +254,15 @@ def test_in_place_and_strided_layouts():
     assert int(out[:, count:].abs().sum()) == 0
 
 
-def test_step_engine_barrier_timeout_is_reported_and_recoverable():
-    """A grid barrier that can never open (fault injected on the host: it
-    waits for one arrival too many) expires after the configured bound; the
-    engine reports BINE_ERR_TIMEOUT and the next call works."""
+@pytest.mark.parametrize("engine", ["steps", "pipelined"])
+def test_step_engine_barrier_timeout_is_reported_and_recoverable(engine):
+    """A wait that can never end (fault injected on the host: a grid barrier
+    waiting for one arrival too many, or a segment waiting for a completion
+    value no segment writes) expires after the configured bound; the engine
+    reports BINE_ERR_TIMEOUT and the next call works."""
     P, count = 16, 16 * 64
     x = np.random.default_rng(6).integers(-1000, 1001, (P, count)).astype(np.int32)
-    comm = make_comm(P, "allreduce", "B", engine="steps")
+    comm = make_comm(P, "allreduce", "B", engine=engine)
     comm.set_step_timeout(200)
     comm.debug_set_barrier_extra(1)
     send = torch.from_numpy(x).cuda()
@@ -421,7 +428,7 @@ def test_allreduce_host_pageable_in_place_and_strided():
     assert np.all(out[:, count:] == 7)
 
 
-@pytest.mark.parametrize("engine", ["fused", "steps"])
+@pytest.mark.parametrize("engine", ["fused", "steps", "pipelined"])
 @pytest.mark.parametrize("coll", bine.COLLS)
 def test_zero_and_ragged_counts(engine, coll):
     """count 0 leaves every output byte as it was; counts below P (1 and
@@ -440,7 +447,36 @@ def test_zero_and_ragged_counts(engine, coll):
         try:
             out = run(comm, coll, x, count, root)
         except bine.Unsupported:
-            assert engine == "steps"
+            assert engine in ("steps", "pipelined")
             continue
         rr = receiving_ranks(coll, P, root)
         assert np.array_equal(out[rr], expected(coll, x, P, count, root)[rr])
+
+
+def test_pipelined_engine_repeated_launches_and_graph_replay():
+    """The pipelined kernel leaves its completion state ready for the next
+    launch: back-to-back calls, and replays of a CUDA graph holding one
+    call, give the exact sums each time, with inputs changed in between."""
+    P, count = 64, 64 * 1000
+    comm = make_comm(P, "allreduce", "B", engine="pipelined")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(8)
+    send = torch.randint(-1000, 1001, (P, count), dtype=torch.int32, device="cuda", generator=g)
+    recv = torch.empty_like(send)
+    for k in range(3):
+        send.add_(k)
+        comm.allreduce(send, recv, count, bine.INT32)
+        comm.synchronize()
+        assert torch.equal(recv, send.sum(0, dtype=torch.int64).to(torch.int32).expand(P, count))
+    stream = torch.cuda.Stream()
+    comm.set_stream(stream)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        comm.allreduce(send, recv, count, bine.INT32)
+    for k in range(3):
+        send.mul_(-1).add_(k)
+        recv.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(recv, send.sum(0, dtype=torch.int64).to(torch.int32).expand(P, count))
+    comm.synchronize()
