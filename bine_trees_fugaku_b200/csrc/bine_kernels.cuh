@@ -812,7 +812,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove
     __shared__ char* s_d[kFlowPieces];
     __shared__ const char* s_a[kFlowPieces];
     __shared__ const char* s_b[kFlowPieces];
-    __shared__ unsigned char s_kind[kFlowPieces];  // bit 0: add, bit 1: 16-byte units
+    __shared__ long long s_nvec[kFlowPieces];      // 16-byte units of the body
+    __shared__ unsigned char s_head[kFlowPieces];  // element units before the body
+    __shared__ unsigned char s_add[kFlowPieces];
     __shared__ long long s_warp[kThreads / 32];
     __shared__ int s_item, s_ok;
     __shared__ unsigned s_target;
@@ -830,9 +832,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove
         const int i = s_item;
         if (i >= nitems) break;
         const FlowItem it = items[i];
-        // Piece table (addresses, unit kind and count; tables only, no data
-        // rows) before the dependency wait, so that it is off the critical
-        // path; then a block scan of the unit counts.
+        // Piece table (addresses; element head, 16-byte body and element
+        // tail; tables only, no data rows) before the dependency wait, so
+        // that it is off the critical path; then a block scan of the unit
+        // counts.  A piece whose destination and sources sit at the same
+        // offset within 16 bytes gets a vector body; any other piece is
+        // all element units.
         const int np = it.pend - it.pbeg;
         long long units = 0;
         if (tid < np) {
@@ -841,13 +846,20 @@ __global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove
             char* d = B.base[m.dst_buf] + (long long)m.dst_rank * B.stride[m.dst_buf] + (m.dst_off + ch.start) * es;
             const char* a = B.base[m.a_buf] + (long long)m.a_rank * B.stride[m.a_buf] + (m.a_off + ch.start) * es;
             const char* b = B.base[m.b_buf] + (long long)m.b_rank * B.stride[m.b_buf] + (m.b_off + ch.start) * es;
-            const long long bytes = ch.n * es;
-            const bool vec = (((uintptr_t)d | (uintptr_t)a | (uintptr_t)(m.add ? b : a)) & 15) == 0 && (bytes & 15) == 0;
-            units = vec ? bytes / 16 : ch.n;
+            const uintptr_t mis = ((uintptr_t)d ^ (uintptr_t)a) | (m.add ? ((uintptr_t)d ^ (uintptr_t)b) : 0);
+            const long long n = ch.n;
+            long long head = n, nvec = 0;
+            if ((mis & 15) == 0) {
+                head = min((long long)((16 - ((uintptr_t)d & 15)) & 15) / es, n);
+                nvec = (n - head) * es / 16;
+            }
+            units = n - nvec * (16 / es) + nvec;
             s_d[tid] = d;
             s_a[tid] = a;
             s_b[tid] = b;
-            s_kind[tid] = (unsigned char)((m.add ? 1 : 0) | (vec ? 2 : 0));
+            s_nvec[tid] = nvec;
+            s_head[tid] = (unsigned char)min(head, 255ll);
+            s_add[tid] = m.add ? 1 : 0;
         }
         if (warp == 0) {
             bool ok = true;
@@ -873,9 +885,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove
         const long long total = s_pref[np];
         int cur = 0;
         for (long long u0 = tid; u0 < total; u0 += (long long)kFlowUnroll * kThreads) {
-            uint4 va[kFlowUnroll], vb[kFlowUnroll];
+            uint4 va[kFlowUnroll], vb[kFlowUnroll];  // a vector, or an element in the low bytes
             char* dp[kFlowUnroll];
-            int kind[kFlowUnroll];
+            int kind[kFlowUnroll];  // -1: none; bit 0: add, bit 1: vector
 #pragma unroll
             for (int k = 0; k < kFlowUnroll; k++) {
                 const long long u = u0 + (long long)k * kThreads;
@@ -890,24 +902,33 @@ __global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove
                         cur = lo;
                     }
                     const long long r = u - s_pref[cur];
-                    const int kd = s_kind[cur];
+                    const long long head = s_head[cur], nvec = s_nvec[cur];
+                    const int add = s_add[cur];
                     // Plain (coherent) loads: other blocks wrote these rows
                     // during this launch.
-                    if (kd & 2) {
-                        kind[k] = kd;
-                        dp[k] = s_d[cur] + r * 16;
-                        va[k] = ld_plain(s_a[cur] + r * 16);
-                        if (kd & 1) vb[k] = ld_plain(s_b[cur] + r * 16);
-                    } else {  // element units (unaligned pieces): done at once
-                        T v = *((volatile const T*)s_a[cur] + r);
-                        if (kd & 1) v = add_exact<T>(v, *((volatile const T*)s_b[cur] + r));
-                        *((T*)s_d[cur] + r) = v;
+                    if (r >= head && r < head + nvec) {
+                        const long long off = head * es + (r - head) * 16;
+                        kind[k] = add | 2;
+                        dp[k] = s_d[cur] + off;
+                        va[k] = ld_plain(s_a[cur] + off);
+                        if (add) vb[k] = ld_plain(s_b[cur] + off);
+                    } else {
+                        const long long e = r < head ? r : r - nvec + nvec * (16 / es);
+                        kind[k] = add;
+                        dp[k] = s_d[cur] + e * es;
+                        *(T*)&va[k] = *((volatile const T*)s_a[cur] + e);
+                        if (add) *(T*)&vb[k] = *((volatile const T*)s_b[cur] + e);
                     }
                 }
             }
 #pragma unroll
-            for (int k = 0; k < kFlowUnroll; k++)
-                if (kind[k] >= 0) *(uint4*)dp[k] = (kind[k] & 1) ? vadd<T>(va[k], vb[k]) : va[k];
+            for (int k = 0; k < kFlowUnroll; k++) {
+                if (kind[k] < 0) continue;
+                if (kind[k] & 2)
+                    *(uint4*)dp[k] = (kind[k] & 1) ? vadd<T>(va[k], vb[k]) : va[k];
+                else
+                    *(T*)dp[k] = (kind[k] & 1) ? add_exact<T>(*(const T*)&va[k], *(const T*)&vb[k]) : *(const T*)&va[k];
+            }
         }
         __syncthreads();
         if (tid == 0) {
