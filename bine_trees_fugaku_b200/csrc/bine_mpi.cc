@@ -18,7 +18,7 @@
 // Two barriers order the steps.  Algorithm selection reads the reference's
 // own environment variables (LIBBINE_<COLL>_ALGO, _ALGO_FAMILY, _DISTANCE,
 // LIBBINE_NUM_PORTS, LIBBINE_DIMENSIONS, LIBBINE_SEGMENT_SIZE;
-// lib/libbine.cc:75-575); BINE_B200_ENGINE=fused|steps and
+// lib/libbine.cc:75-575); BINE_B200_ENGINE=fused|steps|pipelined and
 // BINE_B200_FLOAT_ORDER=reference|fast pick the engine.  Calls the engine
 // cannot take (another communicator, another op or datatype, uneven
 // reduce_scatter counts, mismatched send/recv types) go to the PMPI_
@@ -144,7 +144,10 @@ int make_comm() {
     }
     if (const char* s = env("LIBBINE_SEGMENT_SIZE")) bine_comm_set_segment(g.comm, atoll(s));
     const char* e = env("BINE_B200_ENGINE");
-    bine_comm_set_engine(g.comm, e && strcmp(e, "steps") == 0 ? BINE_ENGINE_STEPS : BINE_ENGINE_FUSED);
+    bine_comm_set_engine(g.comm, !e ? BINE_ENGINE_FUSED
+                                    : strcmp(e, "steps") == 0     ? BINE_ENGINE_STEPS
+                                    : strcmp(e, "pipelined") == 0 ? BINE_ENGINE_PIPELINED
+                                                                  : BINE_ENGINE_FUSED);
     set_float_order_from_env();
     for (int c = 0; c < 8; c++) {
         char key[64];
