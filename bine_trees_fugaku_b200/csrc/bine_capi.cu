@@ -420,7 +420,7 @@ int get_dev_steps(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSt
 
 static_assert(sizeof(FlowPiece) == sizeof(dev::StepChunk), "piece layouts differ");
 static_assert(sizeof(FlowItem) == sizeof(dev::FlowItem), "item layouts differ");
-static_assert(kFlowMaxPieces <= dev::kFlowPieces, "items hold more pieces than the kernel's table");
+static_assert(dev::kFlowPieces <= kFlowMaxPieces, "the kernel's piece table exceeds the planner's bound");
 
 // Item sizing of the pipelined engine: about `target_items` items per level
 // (four per SM, one per resident block), of 4 KiB at least, in whole 4 KiB
@@ -433,11 +433,12 @@ static_assert(kFlowMaxPieces <= dev::kFlowPieces, "items hold more pieces than t
 // 8 and 16 per SM gave 0.91x, 0.80x, 0.82x and 0.91x, and a 1 KiB minimum
 // 0.79x.
 constexpr int64_t kFlowMaxItemBytes = 1 << 20;
-constexpr int kFlowItemsPerSm = 4;
+constexpr int kFlowItemsPerSm = dev::kFlowBlocksPerSm;
 
 void flow_plan(const Schedule& s, int P, int es, long long segment_bytes, int target_items, FlowPlan* fp) {
     const int64_t piece = segment_bytes > 0 ? std::max<int64_t>(16, segment_bytes / es) : 0;
-    build_flow(s, P, piece, std::max<int64_t>(1, 4096 / es), kFlowMaxItemBytes / es, target_items, fp);
+    build_flow(s, P, piece, std::max<int64_t>(1, 4096 / es), kFlowMaxItemBytes / es, target_items, dev::kFlowPieces,
+               fp);
 }
 
 int get_dev_flow(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSteps>* steps,
@@ -1006,11 +1007,11 @@ int launch_flow(bine_comm_t c, const DevSteps& d, const DevFlow& f, const char* 
     B.stride[kBufRecv] = ost;
     B.stride[kBufTmp] = (long long)tmp_stride;
     int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_flow<T>, dev::kThreads, 0));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_flow<T>, dev::kFlowThreads, 0));
     // Resident blocks only: the waits need no co-residency (every dependency
     // was handed out earlier), but blocks beyond that would only queue.
     const int blocks = std::max(1, std::min(std::max(1, per_sm) * c->num_sms, f.nitems));
-    dev::k_flow<T><<<blocks, dev::kThreads, 0, c->stream>>>(B, d.moves, f.pieces, f.items, f.nitems, f.deps,
+    dev::k_flow<T><<<blocks, dev::kFlowThreads, 0, c->stream>>>(B, d.moves, f.pieces, f.items, f.nitems, f.deps,
                                                              f.level_items, f.nlevels, f.done, f.ctl, c->status,
                                                              c->step_timeout_ns, c->barrier_extra);
     CUDA_TRY(cudaGetLastError());

@@ -772,7 +772,9 @@ __global__ void __launch_bounds__(kThreads) k_steps(StepBufs B, const StepMove* 
 struct FlowItem {
     int32_t pbeg, pend, dbeg, dend, level, pad;
 };
-constexpr int kFlowPieces = 256;  // pieces per item, at most one per thread
+constexpr int kFlowThreads = 256;                 // threads per block of k_flow
+constexpr int kFlowBlocksPerSm = 1024 / kFlowThreads;  // resident blocks at 64 registers
+constexpr int kFlowPieces = kFlowThreads;         // pieces per item, at most one per thread
 constexpr int kFlowUnroll = 4;    // 16-byte units in flight per thread
 
 __device__ __forceinline__ bool flow_wait(int dep, const unsigned* done, const unsigned* ctl,
@@ -801,7 +803,7 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 // Completion is a release store after the block barrier (release is
 // cumulative over the block's writes), read with acquire loads.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove* __restrict__ moves,
+__global__ void __launch_bounds__(kFlowThreads, kFlowBlocksPerSm) k_flow(StepBufs B, const StepMove* __restrict__ moves,
                                                       const StepChunk* __restrict__ pieces,
                                                       const FlowItem* __restrict__ items, int nitems,
                                                       const int* __restrict__ deps,
@@ -815,7 +817,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove
     __shared__ long long s_nvec[kFlowPieces];      // 16-byte units of the body
     __shared__ unsigned char s_head[kFlowPieces];  // element units before the body
     __shared__ unsigned char s_add[kFlowPieces];
-    __shared__ long long s_warp[kThreads / 32];
+    __shared__ long long s_warp[kFlowThreads / 32];
     __shared__ int s_item, s_ok;
     __shared__ unsigned s_target;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -884,13 +886,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_flow(StepBufs B, const StepMove
         if (!s_ok) break;  // a wait expired; the status is recorded
         const long long total = s_pref[np];
         int cur = 0;
-        for (long long u0 = tid; u0 < total; u0 += (long long)kFlowUnroll * kThreads) {
+        for (long long u0 = tid; u0 < total; u0 += (long long)kFlowUnroll * kFlowThreads) {
             uint4 va[kFlowUnroll], vb[kFlowUnroll];  // a vector, or an element in the low bytes
             char* dp[kFlowUnroll];
             int kind[kFlowUnroll];  // -1: none; bit 0: add, bit 1: vector
 #pragma unroll
             for (int k = 0; k < kFlowUnroll; k++) {
-                const long long u = u0 + (long long)k * kThreads;
+                const long long u = u0 + (long long)k * kFlowThreads;
                 kind[k] = -1;
                 if (u < total) {
                     if (!(u >= s_pref[cur] && u < s_pref[cur + 1])) {

@@ -1900,8 +1900,9 @@ void flow_cover(FlowRow& row, int64_t s, int64_t e, F f) {
 }  // namespace
 
 void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
-                int target_items, FlowPlan* out) {
+                int target_items, int max_pieces, FlowPlan* out) {
     *out = FlowPlan();
+    max_pieces = std::max(1, std::min(max_pieces, kFlowMaxPieces));
     const bool auto_pieces = piece_elems <= 0;
     target_items = std::max(1, target_items);
     min_item_elems = std::max<int64_t>(1, min_item_elems);
@@ -1928,7 +1929,7 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
             for (int64_t st = 0; st < m.n; st += piece_elems) {
                 const int64_t n = std::min(piece_elems, m.n - st);
                 if (nitems == 0 || cur + n > item_elems ||
-                    out->items.back().pend - out->items.back().pbeg >= kFlowMaxPieces) {
+                    out->items.back().pend - out->items.back().pbeg >= max_pieces) {
                     const int32_t p = (int32_t)out->pieces.size();
                     out->items.push_back(FlowItem{p, p, 0, 0, (int32_t)l, 0});
                     nitems++;

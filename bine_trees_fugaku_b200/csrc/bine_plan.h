@@ -166,7 +166,7 @@ class Planner {
 
 // Dataflow form of a schedule, for the pipelined engine.  Every move is cut
 // into pieces of at most `piece_elems` elements; consecutive pieces of one
-// level are packed into items (at most kFlowMaxPieces pieces and about
+// level are packed into items (at most `max_pieces` <= kFlowMaxPieces pieces and about
 // level elements / `target_items` elements each, never below
 // `min_item_elems` unless the level is smaller).  With piece_elems <= 0 the
 // pieces take the item size of their level, rounded up to a multiple of
@@ -202,7 +202,7 @@ struct FlowPlan {
 // level-by-level execution, the planner emits levels whose moves are
 // independent.
 void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
-                int target_items, FlowPlan* out);
+                int target_items, int max_pieces, FlowPlan* out);
 
 // Per-link byte counts of a message list on the torus: 2 * ndims directed
 // links per node, index (node * ndims + d) * 2 + (dir > 0 ? 0 : 1).
