@@ -744,8 +744,9 @@ def run_dropin_suite(args):
             "unit": "GB/s (algorithmic)", **out, "cores": os.cpu_count(),
             "config": {"workload": WORKLOAD, "P": P_RANKS, "count_per_rank": COUNT,
                        "harness": "oracle/ref_harness.cc: P forked ranks, bench.cc timing",
-                       "engine": "PMPI layer: rows gathered in node-shared pinned memory, "
-                                 "bine_allreduce_host pipeline, rows scattered back"}}
+                       "engine": "PMPI layer: rows deposited into node-shared pinned memory, the "
+                                 "bine_allreduce_host_hooked pipeline taking each column window as soon as "
+                                 "every row holds it, rows collected as windows return"}}
     if "gbs" in out.get("reference", {}) and "gbs" in out.get("engine_pmpi", {}):
         line["speedup"] = out["engine_pmpi"]["gbs"] / out["reference"]["gbs"]
     print(json.dumps(line))

@@ -224,6 +224,7 @@ struct bine_comm_s {
     // and the device staging area (2 slots x input and output windows).
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t ev_in[2] = {}, ev_reduced[2] = {}, ev_out[2] = {}, ev_start = nullptr;
+    std::vector<cudaEvent_t> ev_window;  // per window, for the after-window hook
     char* stage = nullptr;
     size_t stage_bytes = 0;
     long long host_window = 32ll << 20;  // bytes of one column window over all ranks
@@ -238,6 +239,7 @@ struct bine_comm_s {
             if (ev_out[s]) cudaEventDestroy(ev_out[s]);
         }
         if (ev_start) cudaEventDestroy(ev_start);
+        for (cudaEvent_t e : ev_window) cudaEventDestroy(e);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (side) cudaStreamDestroy(side);
@@ -1185,7 +1187,8 @@ int launch_tree_window(bine_comm_t c, const DevTrees& d, const DevTrees::Windows
 // i-1 run at once, so both PCIe directions stay busy.  The fused kernels do
 // the reduction (exact trees with windowed tiles in the reference float
 // order), so results equal bine_allreduce's.
-int allreduce_host(bine_comm_t c, const void* sendbuf, void* recvbuf, long long count, int dt) {
+int allreduce_host(bine_comm_t c, const void* sendbuf, void* recvbuf, long long count, int dt,
+                   bine_window_hook_t before = nullptr, bine_window_hook_t after = nullptr, void* user = nullptr) {
     const int es = dtype_size(dt);
     if (es < 0) return fail(BINE_ERR_ARG, "invalid datatype");
     if (count < 0) return fail(BINE_ERR_ARG, "negative count");
@@ -1237,16 +1240,49 @@ int allreduce_host(bine_comm_t c, const void* sendbuf, void* recvbuf, long long 
         rc = window_tiles(c, *trees, W, count, &win);
         if (rc) return rc;
     }
+    const long long nwin = (count + W - 1) / W;
+    if (after)
+        while ((long long)c->ev_window.size() < nwin) {
+            cudaEvent_t e;
+            CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            c->ev_window.push_back(e);
+        }
+    // After-window hook: windows whose output copy has ended, in order
+    // (without waiting unless `wait`).
+    long long issued = 0, reported = 0;
+    auto report = [&](bool wait) -> int {
+        while (after && reported < issued) {
+            const cudaError_t q = wait ? cudaEventSynchronize(c->ev_window[reported])
+                                       : cudaEventQuery(c->ev_window[reported]);
+            if (q == cudaErrorNotReady) return BINE_SUCCESS;
+            CUDA_TRY(q);
+            const long long c0 = reported * W;
+            if (after(user, c0, std::min(W, count - c0)) != 0)
+                return fail(BINE_ERR_ABORTED, "the after-window hook abandoned the call");
+            reported++;
+        }
+        return BINE_SUCCESS;
+    };
+    // An abandoned call still lets the copies in flight end before its
+    // buffers go back to the caller.
+    auto abandon = [&](int code) {
+        cudaStreamSynchronize(c->h2d);
+        cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->d2h);
+        return code;
+    };
     // The pipeline starts after the work already queued on the
     // communicator's stream and ends on it, so the call is stream-ordered.
     CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
     CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_start, 0));
-    const long long nwin = (count + W - 1) / W;
     for (long long i = 0; i < nwin; i++) {
         const int s = (int)(i & 1);
         const long long c0 = i * W, w = std::min(W, count - c0);
         char* in_s = c->stage + (size_t)(2 * s) * slot;
         char* out_s = c->stage + (size_t)(2 * s + 1) * slot;
+        if ((rc = report(false)) != BINE_SUCCESS) return abandon(rc);
+        if (before && before(user, c0, w) != 0)
+            return abandon(fail(BINE_ERR_ABORTED, "the before-window hook abandoned the call"));
         if (i >= 2) CUDA_TRY(cudaStreamWaitEvent(c->h2d, c->ev_reduced[s], 0));  // input slot consumed
         CUDA_TRY(cudaMemcpy2DAsync(in_s, pitch, (const char*)sendbuf + c0 * es, ist, w * es, P,
                                    cudaMemcpyHostToDevice, c->h2d));
@@ -1268,8 +1304,11 @@ int allreduce_host(bine_comm_t c, const void* sendbuf, void* recvbuf, long long 
         CUDA_TRY(cudaMemcpy2DAsync((char*)recvbuf + c0 * es, ost, out_s, pitch, w * es, P, cudaMemcpyDeviceToHost,
                                    c->d2h));
         CUDA_TRY(cudaEventRecord(c->ev_out[s], c->d2h));
+        if (after) CUDA_TRY(cudaEventRecord(c->ev_window[i], c->d2h));
+        issued = i + 1;
     }
     CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_out[(nwin - 1) & 1], 0));
+    if ((rc = report(true)) != BINE_SUCCESS) return abandon(rc);
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return BINE_SUCCESS;
 }
@@ -1736,6 +1775,14 @@ int bine_allreduce_host(const void* sendbuf, void* recvbuf, int count, bine_data
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
     return allreduce_host(comm, sendbuf, recvbuf, count, datatype);
+}
+
+int bine_allreduce_host_hooked(const void* sendbuf, void* recvbuf, int count, bine_datatype_t datatype,
+                               bine_op_t op, bine_comm_t comm, bine_window_hook_t before_window,
+                               bine_window_hook_t after_window, void* user) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (op != BINE_SUM) return fail(BINE_ERR_ARG, "only BINE_SUM is supported");
+    return allreduce_host(comm, sendbuf, recvbuf, count, datatype, before_window, after_window, user);
 }
 
 int bine_reduce_scatter(const void* sendbuf, void* recvbuf, const int* recvcounts, bine_datatype_t datatype,

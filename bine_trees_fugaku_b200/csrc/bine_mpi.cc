@@ -11,11 +11,15 @@
 //   1. Every rank copies its send buffer into its row of a node-shared,
 //      GPU-pinned array (POSIX shared memory, created at MPI_Init by rank 0
 //      and grown collectively when a call needs more).
-//   2. Rank 0 runs the collective through the C ABI (bine_allreduce_host
-//      for allreduce, otherwise one copy in, the device call, one copy out).
+//   2. Rank 0 runs the collective through the C ABI (one copy in, the
+//      device call, one copy out).
 //   3. Every rank copies its row of the result back.
 //
-// Two barriers order the steps.  Algorithm selection reads the reference's
+// Two barriers order the steps.  MPI_Allreduce overlaps them instead: the
+// ranks publish how many columns of their rows they have deposited, rank 0
+// runs bine_allreduce_host_hooked, whose column windows start as soon as
+// every row holds them, publishes how many output columns have reached host
+// memory, and the ranks collect behind it.  Algorithm selection reads the reference's
 // own environment variables (LIBBINE_<COLL>_ALGO, _ALGO_FAMILY, _DISTANCE,
 // LIBBINE_NUM_PORTS, LIBBINE_DIMENSIONS, LIBBINE_SEGMENT_SIZE;
 // lib/libbine.cc:75-575); BINE_B200_ENGINE=fused|steps|pipelined and
@@ -30,7 +34,9 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sched.h>
 #include <sys/mman.h>
+#include <time.h>
 #include <unistd.h>
 
 #include <algorithm>
@@ -47,12 +53,22 @@ struct Header {  // written by rank 0 between the two barriers
 };
 constexpr size_t kHeader = 256;
 
+// Control words of the overlapped allreduce, after the header, one cache
+// line each: [0] output columns in host memory (rank 0), [1] the call rank
+// 0 abandoned, [2 + r] input columns rank r has deposited.  Words pack
+// (call sequence & 0xffffff) << 40 | columns.
+constexpr size_t kLine = 64;
+size_t ctl_bytes(int P) { return ((size_t)(2 + P) * kLine + 4095) / 4096 * 4096; }
+constexpr int kSeqShift = 40;
+constexpr uint64_t kColMask = (1ull << kSeqShift) - 1;
+
 struct State {
     int rank = -1, size = 0;
     char* shm = nullptr;  // Header, then the input rows, then the output rows
     size_t shm_bytes = 0;
     int generation = 0;
     bool pinned = false;
+    uint64_t seq = 0;            // overlapped allreduce calls so far (the same on every rank)
     bine_comm_t comm = nullptr;  // rank 0 only
     char* dev = nullptr;         // rank 0: device rows (input, then output)
     size_t dev_bytes = 0;
@@ -175,7 +191,7 @@ int make_comm() {
 
 // Collective over MPI_COMM_WORLD: every rank asks for the same size.
 int ensure_shm(size_t need) {
-    need += kHeader;
+    need += kHeader + ctl_bytes(g.size);
     if (g.shm && g.shm_bytes >= need) return MPI_SUCCESS;
     const size_t page = (size_t)sysconf(_SC_PAGESIZE);
     size_t bytes = std::max<size_t>({need, 2 * g.shm_bytes, (size_t)64 << 20});
@@ -219,7 +235,34 @@ int ensure_shm(size_t need) {
 }
 
 Header* header() { return reinterpret_cast<Header*>(g.shm); }
-char* in_rows() { return g.shm + kHeader; }
+char* in_rows() { return g.shm + kHeader + ctl_bytes(g.size); }
+uint64_t* ctl_word(int i) { return reinterpret_cast<uint64_t*>(g.shm + kHeader + (size_t)i * kLine); }
+uint64_t pack(uint64_t seq, long long cols) { return ((seq & 0xffffff) << kSeqShift) | (uint64_t)cols; }
+uint64_t load(int i) { return __atomic_load_n(ctl_word(i), __ATOMIC_ACQUIRE); }
+void publish(int i, uint64_t v) { __atomic_store_n(ctl_word(i), v, __ATOMIC_RELEASE); }
+
+// Columns of call `seq` a progress word reports (-1: another call's word).
+long long columns(uint64_t v, uint64_t seq) {
+    return (v >> kSeqShift) == (seq & 0xffffff) ? (long long)(v & kColMask) : -1;
+}
+
+// Waits until `ready()` holds; false if rank 0 abandoned call `seq` or two
+// minutes pass (a rank that died).  Spins briefly, then sleeps 20 us at a
+// time so that waiting ranks leave the cores to the ranks still copying.
+template <typename Ready>
+bool wait_until(Ready ready, uint64_t seq) {
+    timespec t0, t;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    for (long spin = 0;; spin++) {
+        if (ready()) return true;
+        if (columns(load(1), seq) >= 0) return false;
+        if (spin < 256) continue;
+        const timespec nap = {0, 20000};
+        nanosleep(&nap, nullptr);
+        clock_gettime(CLOCK_MONOTONIC, &t);
+        if (t.tv_sec - t0.tv_sec > 120) return false;
+    }
+}
 
 int ensure_dev(size_t bytes) {
     if (g.dev_bytes >= bytes) return BINE_SUCCESS;
@@ -231,9 +274,9 @@ int ensure_dev(size_t bytes) {
     return BINE_SUCCESS;
 }
 
-// Rank 0: runs one collective over the shared rows.  `in_row`/`out_row`
-// are the per-rank row bytes; the output rows follow the input rows (bcast
-// is in place: its result lands in the input rows).
+// Rank 0: runs one collective other than allreduce over the shared rows.
+// `in_row`/`out_row` are the per-rank row bytes; the output rows follow the
+// input rows (bcast is in place: its result lands in the input rows).
 int leader_run(int coll, int count, int dt, int root, size_t in_row, size_t out_row) {
     int rc = make_comm();
     if (rc) return rc;
@@ -242,38 +285,34 @@ int leader_run(int coll, int count, int dt, int root, size_t in_row, size_t out_
     char* hout = hin + P * in_row;
     bine_comm_set_layout(g.comm, 0, 0);
     for (int attempt = 0; attempt < 2; attempt++) {
-        if (coll == BINE_COLL_ALLREDUCE) {
-            rc = bine_allreduce_host(hin, hout, count, (bine_datatype_t)dt, BINE_SUM, g.comm);
-        } else {
-            rc = ensure_dev(P * (in_row + out_row));
-            if (rc) return rc;
-            char* din = g.dev;
-            char* dout = g.dev + P * in_row;
-            if (cudaMemcpy(din, hin, P * in_row, cudaMemcpyHostToDevice) != cudaSuccess) return BINE_ERR_CUDA;
-            const bine_datatype_t t = (bine_datatype_t)dt;
-            std::vector<int> counts;
-            switch (coll) {
-            case BINE_COLL_REDUCE_SCATTER:
-                counts.assign(P, count);
-                rc = bine_reduce_scatter(din, dout, counts.data(), t, BINE_SUM, g.comm);
-                break;
-            case BINE_COLL_ALLGATHER: rc = bine_allgather(din, count, t, dout, count, t, g.comm); break;
-            case BINE_COLL_BCAST:
-                rc = bine_bcast(din, count, t, root, g.comm);
-                dout = din;
-                break;
-            case BINE_COLL_REDUCE: rc = bine_reduce(din, dout, count, t, BINE_SUM, root, g.comm); break;
-            case BINE_COLL_ALLTOALL: rc = bine_alltoall(din, count, t, dout, count, t, g.comm); break;
-            case BINE_COLL_SCATTER: rc = bine_scatter(din, count, t, dout, count, t, root, g.comm); break;
-            case BINE_COLL_GATHER: rc = bine_gather(din, count, t, dout, count, t, root, g.comm); break;
-            default: rc = BINE_ERR_ARG;
-            }
-            if (rc == BINE_SUCCESS) rc = bine_comm_synchronize(g.comm);
-            char* hdst = coll == BINE_COLL_BCAST ? hin : hout;
-            const size_t nbytes = P * (coll == BINE_COLL_BCAST ? in_row : out_row);
-            if (rc == BINE_SUCCESS && cudaMemcpy(hdst, dout, nbytes, cudaMemcpyDeviceToHost) != cudaSuccess)
-                rc = BINE_ERR_CUDA;
+        rc = ensure_dev(P * (in_row + out_row));
+        if (rc) return rc;
+        char* din = g.dev;
+        char* dout = g.dev + P * in_row;
+        if (cudaMemcpy(din, hin, P * in_row, cudaMemcpyHostToDevice) != cudaSuccess) return BINE_ERR_CUDA;
+        const bine_datatype_t t = (bine_datatype_t)dt;
+        std::vector<int> counts;
+        switch (coll) {
+        case BINE_COLL_REDUCE_SCATTER:
+            counts.assign(P, count);
+            rc = bine_reduce_scatter(din, dout, counts.data(), t, BINE_SUM, g.comm);
+            break;
+        case BINE_COLL_ALLGATHER: rc = bine_allgather(din, count, t, dout, count, t, g.comm); break;
+        case BINE_COLL_BCAST:
+            rc = bine_bcast(din, count, t, root, g.comm);
+            dout = din;
+            break;
+        case BINE_COLL_REDUCE: rc = bine_reduce(din, dout, count, t, BINE_SUM, root, g.comm); break;
+        case BINE_COLL_ALLTOALL: rc = bine_alltoall(din, count, t, dout, count, t, g.comm); break;
+        case BINE_COLL_SCATTER: rc = bine_scatter(din, count, t, dout, count, t, root, g.comm); break;
+        case BINE_COLL_GATHER: rc = bine_gather(din, count, t, dout, count, t, root, g.comm); break;
+        default: rc = BINE_ERR_ARG;
         }
+        if (rc == BINE_SUCCESS) rc = bine_comm_synchronize(g.comm);
+        char* hdst = coll == BINE_COLL_BCAST ? hin : hout;
+        const size_t nbytes = P * (coll == BINE_COLL_BCAST ? in_row : out_row);
+        if (rc == BINE_SUCCESS && cudaMemcpy(hdst, dout, nbytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = BINE_ERR_CUDA;
         // A float sum whose reference order does not exist for this case
         // (the reference fails there) is computed in the FAST order.
         if (rc == BINE_ERR_UNSUPPORTED && attempt == 0 && (dt == BINE_FLOAT || dt == BINE_DOUBLE)) {
@@ -284,6 +323,96 @@ int leader_run(int coll, int count, int dt, int root, size_t in_row, size_t out_
     }
     set_float_order_from_env();
     return rc;
+}
+
+// MPI_Allreduce with the three phases overlapped.  Every rank deposits its
+// row in chunks and publishes its progress; rank 0 runs the host pipeline,
+// whose before-window hook deposits rank 0's own columns and waits for every
+// row's, and whose after-window hook collects rank 0's columns and
+// publishes the output progress; the other ranks collect behind it.  A
+// rank's next call can only reuse the rows after every rank finished
+// collecting this one: rank 0 reads a window only once every rank has
+// deposited it for the next call.
+struct Overlap {
+    uint64_t seq;
+    int P;
+    size_t es, row;  // element and row bytes
+    const char* src;
+    char* dst;
+    long long deposited = 0;  // rank 0's own columns in its row
+};
+
+int before_window(void* u, long long first, long long n) {
+    Overlap& o = *static_cast<Overlap*>(u);
+    const long long end = first + n;
+    if (end > o.deposited) {
+        memcpy(in_rows() + o.deposited * o.es, o.src + o.deposited * o.es, (size_t)(end - o.deposited) * o.es);
+        o.deposited = end;
+    }
+    for (int r = 1; r < o.P; r++)
+        if (!wait_until([&] { return columns(load(2 + r), o.seq) >= end; }, o.seq)) return 1;
+    return 0;
+}
+
+int after_window(void* u, long long first, long long n) {
+    Overlap& o = *static_cast<Overlap*>(u);
+    memcpy(o.dst + first * o.es, in_rows() + (size_t)o.P * o.row + first * o.es, (size_t)n * o.es);
+    publish(0, pack(o.seq, first + n));
+    return 0;
+}
+
+int allreduce_overlapped(int count, int dt, size_t es, const void* src, void* dst) {
+    const size_t P = (size_t)g.size, row = (size_t)count * es;
+    int rc = ensure_shm(2 * P * row);
+    if (rc != MPI_SUCCESS) return rc;
+    do {
+        ++g.seq;
+    } while ((g.seq & 0xffffff) == 0);  // a never-written (zero) word must not match
+    const uint64_t seq = g.seq;
+    if (g.rank != 0) {
+        // Deposit in chunks of 256 KiB, then collect behind rank 0.
+        char* mine = in_rows() + (size_t)g.rank * row;
+        const long long chunk = std::max<long long>(1, (256 << 10) / (long long)es);
+        for (long long c0 = 0; c0 < count; c0 += chunk) {
+            const long long c1 = std::min<long long>(count, c0 + chunk);
+            memcpy(mine + c0 * es, (const char*)src + c0 * es, (size_t)(c1 - c0) * es);
+            publish(2 + g.rank, pack(seq, c1));
+        }
+        if (count == 0) publish(2 + g.rank, pack(seq, 0));
+        const char* out = in_rows() + P * row + (size_t)g.rank * row;
+        long long have = 0;
+        while (have < count) {
+            long long done = -1;
+            if (!wait_until([&] { return (done = columns(load(0), seq)) > have; }, seq)) break;
+            memcpy((char*)dst + have * es, out + have * es, (size_t)(done - have) * es);
+            have = done;
+        }
+        if (have == count) return MPI_SUCCESS;
+        if (columns(load(1), seq) < 0) fprintf(stderr, "bine_mpi: rank %d: rank 0 stopped answering\n", g.rank);
+        return MPI_ERR_OTHER;
+    }
+    Overlap o{seq, (int)P, es, row, (const char*)src, (char*)dst};
+    rc = make_comm();
+    if (rc == BINE_SUCCESS) {
+        bine_comm_set_layout(g.comm, 0, 0);
+        char* hin = in_rows();
+        rc = bine_allreduce_host_hooked(hin, hin + P * row, count, (bine_datatype_t)dt, BINE_SUM, g.comm,
+                                        before_window, after_window, &o);
+        // A float sum whose reference order does not exist for this case
+        // (the reference fails there) is computed in the FAST order.
+        if (rc == BINE_ERR_UNSUPPORTED && (dt == BINE_FLOAT || dt == BINE_DOUBLE)) {
+            bine_comm_set_float_order(g.comm, BINE_ORDER_FAST);
+            rc = bine_allreduce_host_hooked(hin, hin + P * row, count, (bine_datatype_t)dt, BINE_SUM, g.comm,
+                                            before_window, after_window, &o);
+        }
+        set_float_order_from_env();
+    }
+    if (rc != BINE_SUCCESS) {
+        fprintf(stderr, "bine_mpi: %s\n", bine_last_error_string());
+        publish(1, pack(seq, 0));  // the other ranks stop waiting
+        return MPI_ERR_OTHER;
+    }
+    return MPI_SUCCESS;
 }
 
 // The three phases every rank runs: deposit its input row, rank 0
@@ -342,10 +471,8 @@ int MPI_Allreduce(const void* sendbuf, void* recvbuf, int count, MPI_Datatype dt
         return PMPI_Allreduce(sendbuf, recvbuf, count, dt, op, comm);
     int es = 0;
     PMPI_Type_size(dt, &es);
-    const size_t row = (size_t)count * es;
     const void* src = sendbuf == MPI_IN_PLACE ? recvbuf : sendbuf;
-    return run_shared(BINE_COLL_ALLREDUCE, count, t, 0, row, row, [&](char* d) { memcpy(d, src, row); },
-                      [&](const char* s) { memcpy(recvbuf, s, row); });
+    return allreduce_overlapped(count, t, (size_t)es, src, recvbuf);
 }
 
 // MPI_Reduce_scatter, lib/libbine.cc:1064 (equal counts, as the reference

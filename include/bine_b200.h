@@ -47,7 +47,8 @@ enum {
     BINE_ERR_CUDA = 3,        /* a CUDA call failed */
     BINE_ERR_TIMEOUT = 4,     /* a bounded device-side wait expired */
     BINE_ERR_NOMEM = 5,       /* device memory exhausted */
-    BINE_ERR_INTERNAL = 6
+    BINE_ERR_INTERNAL = 6,
+    BINE_ERR_ABORTED = 7      /* a caller's window hook abandoned the call */
 };
 
 /* Collectives, for bine_comm_set_algo() and the planning queries. */
@@ -150,6 +151,24 @@ int bine_allreduce(const void *sendbuf, void *recvbuf, int count, bine_datatype_
  * setting; float sums follow the communicator's float order). */
 int bine_allreduce_host(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype, bine_op_t op,
                         bine_comm_t comm);
+
+/* bine_allreduce_host with the caller in the pipeline, for callers whose
+ * input rows fill while the call runs and whose output rows drain as they
+ * arrive (the PMPI layer: every MPI rank deposits its row into shared pinned
+ * memory and collects its result row from it).  The call moves column
+ * windows [first, first + count) of all rows in increasing order:
+ * before_window(user, first, count) runs before a window's input columns
+ * are copied to the GPU and returns once every row holds them;
+ * after_window(user, first, count) runs once that window's output columns
+ * of every row are in host memory.  A nonzero return from either hook
+ * abandons the call (after the copies in flight end) with
+ * BINE_ERR_ABORTED.  Either hook may be NULL.  Results equal
+ * bine_allreduce_host's.  No counterpart in the reference: its MPI layer
+ * has no host pipeline. */
+typedef int (*bine_window_hook_t)(void *user, long long first, long long count);
+int bine_allreduce_host_hooked(const void *sendbuf, void *recvbuf, int count, bine_datatype_t datatype,
+                               bine_op_t op, bine_comm_t comm, bine_window_hook_t before_window,
+                               bine_window_hook_t after_window, void *user);
 
 /* Bytes of one column window of bine_allreduce_host over all ranks
  * (default 32 MiB; at least 4 KiB).  Smaller windows shorten the pipeline's
