@@ -20,7 +20,9 @@ from .build import LIB_PATH
 
 INT32, INT64, FLOAT, DOUBLE, CHAR = 0, 1, 2, 3, 4
 SUM = 0
-SUCCESS, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_INTERNAL = range(7)
+SUCCESS, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_INTERNAL, ERR_ABORTED = range(8)
+# bine_window_hook_t: (user, first column, columns) -> 0 to go on
+WINDOW_HOOK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong)
 ENGINE_FUSED, ENGINE_STEPS, ENGINE_PIPELINED = 0, 1, 2
 ORDER_REFERENCE, ORDER_FAST = 0, 1
 FAMILY = {"BINE": 1, "RECDOUB": 2, "BRUCK": 3}
@@ -112,6 +114,8 @@ def lib():
         "bine_debug_set_barrier_extra": [vp, ctypes.c_uint],
         "bine_comm_set_tree_split": [vp, ctypes.c_int],
         "bine_allreduce_host": [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp],
+        "bine_allreduce_host_hooked": [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, WINDOW_HOOK, WINDOW_HOOK,
+                                       vp],
         "bine_comm_set_host_window": [vp, ctypes.c_longlong],
         "bine_comm_synchronize": [vp],
         "bine_allreduce": [vp, vp, i, i, i, vp],
@@ -271,6 +275,17 @@ class Comm:
         """bine_allreduce_host: host (CPU) tensors or numpy arrays, pinned
         for full bandwidth; returns when recvbuf holds the result."""
         check(lib().bine_allreduce_host(_host_ptr(sendbuf), _host_ptr(recvbuf), count, datatype, op, self._h))
+
+    def allreduce_host_hooked(self, sendbuf, recvbuf, count, datatype, before=None, after=None, op=SUM):
+        """bine_allreduce_host_hooked: `before(first, n)` runs before the
+        input columns [first, first + n) go to the GPU, `after(first, n)`
+        once those output columns are in host memory; a truthy return
+        abandons the call (BineError with code ERR_ABORTED)."""
+        def wrap(fn):
+            return WINDOW_HOOK(lambda _u, first, n: 1 if fn(first, n) else 0) if fn else WINDOW_HOOK()
+        hb, ha = wrap(before), wrap(after)  # kept alive for the call
+        check(lib().bine_allreduce_host_hooked(_host_ptr(sendbuf), _host_ptr(recvbuf), count, datatype, op, self._h,
+                                               hb, ha, None))
 
     def reduce_scatter(self, sendbuf, recvbuf, recvcounts, datatype, op=SUM):
         rc = (ctypes.c_int * self.nranks)(*recvcounts)

@@ -480,3 +480,33 @@ def test_pipelined_engine_repeated_launches_and_graph_replay():
         torch.cuda.synchronize()
         assert torch.equal(recv, send.sum(0, dtype=torch.int64).to(torch.int32).expand(P, count))
     comm.synchronize()
+
+
+def test_hooked_host_allreduce_runs_windows_in_order_and_can_be_abandoned():
+    """bine_allreduce_host_hooked: the hooks see consecutive column windows
+    covering the call, before-window ahead of after-window; results equal
+    bine_allreduce_host's; a hook that returns nonzero abandons the call
+    with BINE_ERR_ABORTED and the next call works."""
+    P, count = 8, 50_000
+    x = torch.randint(-1000, 1001, (P, count), dtype=torch.int32).pin_memory()
+    plain, hooked = torch.empty_like(x).pin_memory(), torch.zeros_like(x).pin_memory()
+    comm = make_comm(P, "allreduce", "B")
+    comm.set_host_window(64 << 10)  # several windows
+    comm.allreduce_host(x, plain, count, bine.INT32)
+    seen = []
+    comm.allreduce_host_hooked(x, hooked, count, bine.INT32, before=lambda f, n: seen.append(("in", f, n)),
+                               after=lambda f, n: seen.append(("out", f, n)))
+    assert torch.equal(hooked, plain)
+    assert torch.equal(plain, x.sum(0, dtype=torch.int64).to(torch.int32).expand(P, count))
+    for kind in ("in", "out"):
+        w = [(f, n) for k, f, n in seen if k == kind]
+        assert len(w) > 2 and w[0][0] == 0 and all(a[0] + a[1] == b[0] for a, b in zip(w, w[1:]))
+        assert w[-1][0] + w[-1][1] == count
+    order = [(k, f) for k, f, _ in seen]
+    assert all(order.index(("in", f)) < order.index(("out", f)) for _, f, _ in seen)
+    with pytest.raises(bine.BineError) as e:
+        comm.allreduce_host_hooked(x, hooked, count, bine.INT32, before=lambda f, n: f > 0)
+    assert e.value.code == bine.ERR_ABORTED
+    hooked.zero_()
+    comm.allreduce_host_hooked(x, hooked, count, bine.INT32)
+    assert torch.equal(hooked, plain)
