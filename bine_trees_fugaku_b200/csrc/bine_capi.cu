@@ -215,6 +215,8 @@ struct bine_comm_s {
     int num_sms = 0;
     char* work = nullptr;
     size_t work_bytes = 0;
+    char* inplace = nullptr;  // staged input rows of in-place step-engine allreduce calls
+    size_t inplace_bytes = 0;
     unsigned* barrier = nullptr;  // [0] arrivals, [1] generation
     int* status = nullptr;
     unsigned long long step_timeout_ns = 5ull * 1000 * 1000 * 1000;
@@ -230,6 +232,7 @@ struct bine_comm_s {
     long long host_window = 32ll << 20;  // bytes of one column window over all ranks
     ~bine_comm_s() {
         cudaFree(work);
+        cudaFree(inplace);
         cudaFree(barrier);
         cudaFree(status);
         cudaFree(stage);
@@ -1083,7 +1086,7 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
     long long se, re;
     row_elems(coll, count, c->P, &se, &re);
     if ((se && !sendbuf) || (re && !recvbuf)) return fail(BINE_ERR_ARG, "null buffer");
-    const long long ist = c->send_stride ? (long long)c->send_stride : se * es;
+    long long ist = c->send_stride ? (long long)c->send_stride : se * es;
     const long long ost = c->recv_stride ? (long long)c->recv_stride : re * es;
     if (ist < se * es || ost < re * es) return fail(BINE_ERR_ARG, "layout stride smaller than a rank row");
     if (count == 0) return BINE_SUCCESS;
@@ -1093,6 +1096,28 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
     char* out = (char*)recvbuf;
     PlanKey k = make_key(c, coll, count, root);
 
+    // In place (MPI_IN_PLACE): the step schedules read a rank's send row in
+    // the same step that writes receive rows (the L butterfly reads its
+    // peer's input while the peer's result is written), which is a race
+    // once the two rows are one.  The step engines therefore take the input
+    // rows from a staged copy; the fused kernels read every input of a tile
+    // before writing it and need none.
+    if ((c->engine == BINE_ENGINE_STEPS || c->engine == BINE_ENGINE_PIPELINED) && coll == kAllreduce &&
+        (const void*)in == (const void*)out) {
+        const size_t pitch = ((size_t)se * es + 255) / 256 * 256, bytes = pitch * (size_t)c->P;
+        if (c->inplace_bytes < bytes) {
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            cudaFree(c->inplace);
+            c->inplace = nullptr;
+            c->inplace_bytes = 0;
+            CUDA_TRY(cudaMalloc(&c->inplace, bytes));
+            c->inplace_bytes = bytes;
+        }
+        CUDA_TRY(cudaMemcpy2DAsync(c->inplace, pitch, in, ist, (size_t)se * es, c->P, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+        in = c->inplace;
+        ist = (long long)pitch;
+    }
     if (c->engine == BINE_ENGINE_STEPS) {
         std::shared_ptr<DevSteps> d;
         rc = get_dev_steps(c, k, es, &d);
@@ -1384,7 +1409,12 @@ int noalloc_run(bine_comm_t c, const Schedule& s, const char* send, long long is
     const size_t off_lb = 256, off_mv = off_lb + round256(lb.size() * sizeof(int));
     const size_t off_ch = off_mv + round256(moves.size() * sizeof(dev::StepMove));
     const size_t off_ws = off_ch + round256(chunks.size() * sizeof(dev::StepChunk));
-    const size_t need = off_ws + tmp_stride * (size_t)c->P;
+    // In place: the input rows are staged after the workspace (the step
+    // schedule would otherwise read rows the same step overwrites).
+    const bool in_place = (const void*)send == (const void*)recv;
+    const size_t in_pitch = round256((size_t)s.send_elems * sizeof(T));
+    const size_t off_in = off_ws + tmp_stride * (size_t)c->P;
+    const size_t need = off_in + (in_place ? in_pitch * (size_t)c->P : 0);
     if (need > kNoAllocScratchBytes)
         return fail(BINE_ERR_NOMEM, "bine_allreduce_noalloc: this call needs " + std::to_string(need) +
                                         " bytes of scratch, more than the fixed " +
@@ -1402,6 +1432,12 @@ int noalloc_run(bine_comm_t c, const Schedule& s, const char* send, long long is
     if (!chunks.empty())
         CUDA_TRY(cudaMemcpyAsync(base + off_ch, chunks.data(), chunks.size() * sizeof(dev::StepChunk),
                                  cudaMemcpyHostToDevice, st));
+    if (in_place) {
+        CUDA_TRY(cudaMemcpy2DAsync(base + off_in, in_pitch, send, ist, (size_t)s.send_elems * sizeof(T), c->P,
+                                   cudaMemcpyDeviceToDevice, st));
+        send = base + off_in;
+        ist = (long long)in_pitch;
+    }
     dev::StepBufs B;
     B.base[kBufSend] = const_cast<char*>(send);
     B.base[kBufRecv] = recv;

@@ -1942,10 +1942,9 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
         }
         out->level_items.push_back(nitems);
     }
-    // Dependencies over rows (buffer, rank); send and receive rows share one
-    // row space.
-    auto row_id = [&](const Region& r) { return (r.buf == kBufTmp ? P : 0) + r.rank; };
-    std::vector<FlowRow> rows(2 * (size_t)P);
+    // Dependencies over rows (buffer, rank).
+    auto row_id = [&](const Region& r) { return (size_t)r.buf * P + r.rank; };
+    std::vector<FlowRow> rows(kNumBufs * (size_t)P);
     std::vector<int32_t> cand;
     for (int32_t i = 0; i < (int32_t)out->items.size(); i++) {
         FlowItem& it = out->items[i];

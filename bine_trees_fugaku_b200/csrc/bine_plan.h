@@ -197,10 +197,10 @@ struct FlowPlan {
     std::vector<int32_t> level_items;  // items per level
 };
 
-// The send and receive rows of a rank are tracked as one row (an in-place
-// call aliases them).  Moves of one level never wait for each other: as in
-// level-by-level execution, the planner emits levels whose moves are
-// independent.
+// Moves of one level never wait for each other: as in level-by-level
+// execution, the planner emits levels whose moves are independent.  The
+// send, receive and workspace rows are distinct (an in-place call's input
+// rows are staged before the schedule runs).
 void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
                 int target_items, int max_pieces, FlowPlan* out);
 

@@ -510,3 +510,25 @@ def test_hooked_host_allreduce_runs_windows_in_order_and_can_be_abandoned():
     hooked.zero_()
     comm.allreduce_host_hooked(x, hooked, count, bine.INT32)
     assert torch.equal(hooked, plain)
+
+
+@pytest.mark.parametrize("engine", ["steps", "pipelined"])
+@pytest.mark.parametrize("variant,P", [("B", 16), ("B", 24), ("L", 4), ("L", 16), ("L", 24), ("B_COALESCE", 12)])
+def test_in_place_allreduce_on_the_step_engines(engine, variant, P):
+    """MPI_IN_PLACE (sendbuf == recvbuf) on the engines that run the
+    reference's schedule: the L butterfly reads a peer's input in the step
+    that writes the peer's result, so the input rows are staged first; two
+    calls in a row give the out-of-place bytes, float32 included."""
+    count = P * 37 + 5
+    for dt, code in ((np.int32, bine.INT32), (np.float32, bine.FLOAT)):
+        rng = np.random.default_rng(P)
+        x = (rng.integers(-1000, 1001, (P, count)) if dt == np.int32 else rng.standard_normal((P, count))).astype(dt)
+        comm = make_comm(P, "allreduce", variant, engine=engine)
+        send = torch.from_numpy(x).cuda()
+        expect = torch.empty_like(send)
+        comm.allreduce(send, expect, count, code)
+        for _ in range(2):
+            buf = send.clone()
+            comm.allreduce(buf, buf, count, code)
+            comm.synchronize()
+            assert torch.equal(buf.view(torch.uint8), expect.view(torch.uint8))

@@ -6,8 +6,8 @@ independently of how the planner derives it:
 
 * the pieces tile every move exactly and items stay within one level;
 * every element-level conflict (read after write, write after write, write
-  after read, with a rank's send and receive rows aliased as in an in-place
-  call) between items of different levels is ordered by a dependency path;
+  after read) between items of different levels is ordered by a dependency
+  path;
 * no two moves of one level conflict (the premise of both step engines);
 * running the items in a random order the dependencies allow gives the
   reference's results, bit for bit.
@@ -91,7 +91,7 @@ def check_conflicts(mv, add, pieces, items, deps):
             a |= (anc[d] | (1 << d)) if d >= 0 else level_all[-d - 1]
         anc[i] = a
         need = set()
-        acc = [t for p in range(pb, pe) for t in touched(mv, add, *pieces[p].tolist(), alias=True)]
+        acc = [t for p in range(pb, pe) for t in touched(mv, add, *pieces[p].tolist(), alias=False)]
         for row, s, e, w in acc:
             if not w:
                 lw, rd = writer.setdefault(row, {}), readers.setdefault(row, {})
@@ -224,3 +224,4 @@ def test_flow_plan_larger_schedules_order_every_conflict(coll, variant, P, count
     mv, n, add, pieces, items, deps = plan(comm, case, 4, 40)
     check_structure(mv, n, pieces, items, deps)
     check_conflicts(mv, add, pieces, items, deps)
+

@@ -72,3 +72,21 @@ def test_noalloc_refuses_calls_that_need_more_than_its_scratch():
     rc = noalloc_allreduce(comm, send, recv, count, bine.FLOAT)
     assert rc == bine.ERR_NOMEM
     assert "scratch" in bine.last_error()
+
+
+def test_noalloc_in_place_matches_out_of_place():
+    """In place (the same buffer for input and result), the input rows are
+    staged in the fixed scratch before the schedule runs; two calls in a
+    row give the out-of-place bytes."""
+    P, count = 16, 16 * 37 + 5
+    comm = bine.Comm(P)
+    comm.set_algo("allreduce", "L")
+    comm.set_stream(torch.cuda.current_stream())
+    x = torch.from_numpy(np.random.default_rng(9).standard_normal((P, count)).astype(np.float32)).cuda()
+    want = torch.zeros_like(x)
+    assert noalloc_allreduce(comm, x, want, count, bine.FLOAT) == bine.SUCCESS, bine.last_error()
+    for _ in range(2):
+        buf = x.clone()
+        assert noalloc_allreduce(comm, buf, buf, count, bine.FLOAT) == bine.SUCCESS, bine.last_error()
+        torch.cuda.synchronize()
+        assert torch.equal(buf, want)
