@@ -835,9 +835,9 @@ __global__ void __launch_bounds__(kFlowThreads, kFlowBlocksPerSm) k_flow(StepBuf
         if (i >= nitems) break;
         const FlowItem it = items[i];
         // Piece table (addresses; element head, 16-byte body and element
-        // tail; tables only, no data rows) before the dependency wait, so
-        // that it is off the critical path; then a block scan of the unit
-        // counts.  A piece whose destination and sources sit at the same
+        // tail; tables only, no data rows) and a block scan of the unit
+        // counts, both before the dependency wait, so that they are off the
+        // critical path.  A piece whose destination and sources sit at the same
         // offset within 16 bytes gets a vector body; any other piece is
         // all element units.
         const int np = it.pend - it.pbeg;
@@ -863,13 +863,6 @@ __global__ void __launch_bounds__(kFlowThreads, kFlowBlocksPerSm) k_flow(StepBuf
             s_head[tid] = (unsigned char)min(head, 255ll);
             s_add[tid] = m.add ? 1 : 0;
         }
-        if (warp == 0) {
-            bool ok = true;
-            for (int d = it.dbeg + lane; d < it.dend && ok; d += 32)
-                ok = flow_wait(deps[d], done, ctl, level_items, target, extra, status, timeout_ns);
-            ok = __all_sync(0xffffffffu, ok);
-            if (lane == 0) s_ok = ok;
-        }
         long long inc = units;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -882,6 +875,15 @@ __global__ void __launch_bounds__(kFlowThreads, kFlowBlocksPerSm) k_flow(StepBuf
         for (int w = 0; w < warp; w++) before += s_warp[w];
         s_pref[tid + 1] = before + inc;
         if (tid == 0) s_pref[0] = 0;
+        // The dependency wait comes last, so that only one block barrier
+        // separates the last dependency's completion from this item's loads.
+        if (warp == 0) {
+            bool ok = true;
+            for (int d = it.dbeg + lane; d < it.dend && ok; d += 32)
+                ok = flow_wait(deps[d], done, ctl, level_items, target, extra, status, timeout_ns);
+            ok = __all_sync(0xffffffffu, ok);
+            if (lane == 0) s_ok = ok;
+        }
         __syncthreads();
         if (!s_ok) break;  // a wait expired; the status is recorded
         const long long total = s_pref[np];
