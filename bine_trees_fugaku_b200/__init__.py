@@ -287,8 +287,21 @@ class Comm:
         check(lib().bine_allreduce_host_hooked(_host_ptr(sendbuf), _host_ptr(recvbuf), count, datatype, op, self._h,
                                                hb, ha, None))
 
+    def _equal_counts(self, count):
+        """ctypes array of nranks copies of `count`, cached: building it per
+        call costs more host time than a small call takes on the GPU."""
+        cache = self.__dict__.setdefault("_counts_cache", {})
+        if count not in cache:
+            if len(cache) > 64:
+                cache.clear()
+            cache[count] = (ctypes.c_int * self.nranks)(*([count] * self.nranks))
+        return cache[count]
+
     def reduce_scatter(self, sendbuf, recvbuf, recvcounts, datatype, op=SUM):
-        rc = (ctypes.c_int * self.nranks)(*recvcounts)
+        if isinstance(recvcounts, ctypes.Array):
+            rc = recvcounts
+        else:
+            rc = (ctypes.c_int * self.nranks)(*recvcounts)
         check(lib().bine_reduce_scatter(_ptr(sendbuf), _ptr(recvbuf), rc, datatype, op, self._h))
 
     def allgather(self, sendbuf, sendcount, sendtype, recvbuf, recvcount, recvtype):
@@ -316,7 +329,7 @@ class Comm:
         if coll == "allreduce":
             return self.allreduce(sendbuf, recvbuf, count, datatype)
         if coll == "reduce_scatter":
-            return self.reduce_scatter(sendbuf, recvbuf, [count] * self.nranks, datatype)
+            return self.reduce_scatter(sendbuf, recvbuf, self._equal_counts(count), datatype)
         if coll == "allgather":
             return self.allgather(sendbuf, count, datatype, recvbuf, count, datatype)
         if coll == "bcast":

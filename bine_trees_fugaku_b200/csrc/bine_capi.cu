@@ -770,14 +770,20 @@ int launch_sum(bine_comm_t c, int mode, const char* in, long long ist, char* out
             // per SM.  Measured on B200 at 4 MiB per rank (GB/s, old rule ->
             // 64 columns): P = 16: 6406 -> 7084; 64: 5726 -> 6194; 256: 5716
             // -> 6347; 1024: 5751 -> 6316.
+            // Below 32 columns a tile has more row groups than that (16 or
+            // 32); only for P of at least two rows per group.
             int cols = P < 16 ? 256 : 64;
-            while (cols > 32 && ncol / cols < 2LL * std::max(1, c->num_sms)) cols /= 2;
+            while (ncol / cols < 2LL * std::max(1, c->num_sms) &&
+                   (cols > 32 || (cols > dev::kSumCols && P >= 2 * (2 * dev::kThreads / cols))))
+                cols /= 2;
             int rc;
             switch (cols) {
             case 256: rc = launch_sum_cols<T, 256>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
             case 128: rc = launch_sum_cols<T, 128>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
             case 64: rc = launch_sum_cols<T, 64>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
-            default: rc = launch_sum_cols<T, 32>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
+            case 32: rc = launch_sum_cols<T, 32>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
+            case 16: rc = launch_sum_cols<T, 16>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
+            default: rc = launch_sum_cols<T, 8>(c, mode, in, ist, out, ost, P, ncol, blk_vec, root); break;
             }
             if (rc) return rc;
             done = ncol * 16 / es;
@@ -941,12 +947,24 @@ int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist,
 
 int launch_copy(bine_comm_t c, int mode, const char* in, long long ist, char* out, long long ost, long long unit,
                 int root, int es) {
-    dev::CopyArgs a{in, ist, out, ost, c->P, root, unit};
+    dev::CopyArgs a{in, ist, out, ost, c->P, root, unit, 1};
     long long pairs = mode == dev::kCopyAlltoall ? (long long)c->P * c->P : (mode == dev::kCopyBcast ? 1 : c->P);
     if (unit == 0) return BINE_SUCCESS;
     const bool vec = aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0 && unit % 16 == 0;
+    // Allgather and bcast store every source vector to P rows.  A call whose
+    // source units would give fewer than half the SMs a block leaves most
+    // of the GPU idle: its rows are then split over threads, enough groups
+    // for two blocks per SM (at least 8 rows each).  Calls that already
+    // reach most SMs stream their stores at full rate unsplit.  Measured
+    // on B200 (int64, us): bcast P = 1024 at 8 KiB per rank 69.7 -> 4.4,
+    // allgather P = 1024 at 32 B 69.8 -> 8.3; allgather P = 1024 at 512 B
+    // (128 blocks) 78 unsplit, 95 split in 3.
+    const long long units = pairs * (vec ? unit / 16 : unit / es);
+    const long long fill = 2LL * dev::kThreads * std::max(1, c->num_sms);
+    if ((mode == dev::kCopyAllgather || mode == dev::kCopyBcast) && 4 * units < fill)
+        a.dgroups = (int)std::max<long long>(1, std::min<long long>(std::max(1, c->P / 8), (fill + units - 1) / units));
     if (vec) {
-        unsigned g = grid_for(c, pairs * (unit / 16));
+        unsigned g = grid_for(c, pairs * (unit / 16) * a.dgroups);
         switch (mode) {
         case dev::kCopyAllgather: dev::k_copy_vec<dev::kCopyAllgather><<<g, dev::kThreads, 0, c->stream>>>(a); break;
         case dev::kCopyBcast: dev::k_copy_vec<dev::kCopyBcast><<<g, dev::kThreads, 0, c->stream>>>(a); break;
@@ -955,7 +973,7 @@ int launch_copy(bine_comm_t c, int mode, const char* in, long long ist, char* ou
         case dev::kCopyGather: dev::k_copy_vec<dev::kCopyGather><<<g, dev::kThreads, 0, c->stream>>>(a); break;
         }
     } else {
-        unsigned g = grid_for(c, pairs * (unit / es));
+        unsigned g = grid_for(c, pairs * (unit / es) * a.dgroups);
 #define BINE_COPY_SCALAR(U)                                                                                          \
     switch (mode) {                                                                                                  \
     case dev::kCopyAllgather: dev::k_copy_scalar<dev::kCopyAllgather, U><<<g, dev::kThreads, 0, c->stream>>>(a); break; \

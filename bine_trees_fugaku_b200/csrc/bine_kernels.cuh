@@ -129,7 +129,7 @@ enum SumMode { kSumAllreduce = 0, kSumReduceScatter = 1, kSumReduce = 2 };
 // block per tile up to 64 blocks per SM, beyond which blocks walk the tiles
 // grid-stride.  `ncol` vector columns per input row; reduce_scatter: `blk`
 // vector columns per destination rank.
-constexpr int kSumCols = 32;  // the narrowest tile
+constexpr int kSumCols = 8;  // the narrowest tile (32 row groups)
 
 template <typename T, int MODE, int COLS>
 __global__ void __launch_bounds__(kThreads) k_sum_vec(const char* __restrict__ in, long long in_stride,
@@ -572,6 +572,7 @@ struct CopyArgs {
     int P;
     int root;
     long long unit;  // bytes per block
+    int dgroups;     // allgather / bcast: destination groups per source vector (>= 1)
 };
 
 template <int MODE>
@@ -600,6 +601,13 @@ __device__ __forceinline__ int copy_ndst(const CopyArgs& a) {
     if (MODE == kCopyBcast) return a.P;
     return 1;
 }
+// Allgather and bcast calls with few source vectors split each vector's
+// destinations over `dgroups` threads (each loads the vector and stores to
+// its share of the rows), so that small calls still fill the GPU.
+template <int MODE>
+__device__ __forceinline__ int copy_groups(const CopyArgs& a) {
+    return (MODE == kCopyAllgather || MODE == kCopyBcast) ? max(1, a.dgroups) : 1;
+}
 template <int MODE>
 __device__ __forceinline__ char* copy_dst(const CopyArgs& a, long long i, int d) {
     if (MODE == kCopyAllgather) return a.out + (long long)d * a.out_stride + i * a.unit;
@@ -615,15 +623,26 @@ __device__ __forceinline__ char* copy_dst(const CopyArgs& a, long long i, int d)
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_copy_vec(CopyArgs a) {
     const long long nvec = a.unit / 16;
-    const long long total = copy_pairs<MODE>(a) * nvec;
     const long long step = (long long)gridDim.x * blockDim.x;
-    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += step) {
-        const long long i = w / nvec, j = w - (w / nvec) * nvec;
-        const uint4 v = ld_stream(copy_src<MODE>(a, i) + j * 16);
-        const int nd = copy_ndst<MODE>(a);
-        for (int d = 0; d < nd; d++) {
-            char* q = copy_dst<MODE>(a, i, d);
-            if (q) st_stream(q + j * 16, v);
+    if constexpr (MODE == kCopyAllgather || MODE == kCopyBcast) {
+        const int G = copy_groups<MODE>(a);
+        const long long per = copy_pairs<MODE>(a) * nvec, total = per * G;
+        for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += step) {
+            const long long gi = G == 1 ? 0 : w / per, r = w - gi * per;
+            const long long i = r / nvec, j = r - i * nvec;
+            const uint4 v = ld_stream(copy_src<MODE>(a, i) + j * 16);
+            const int nd = copy_ndst<MODE>(a);
+            const int d0 = (int)(nd * gi / G), d1 = (int)(nd * (gi + 1) / G);
+            for (int d = d0; d < d1; d++) {
+                char* q = copy_dst<MODE>(a, i, d);
+                if (q) st_stream(q + j * 16, v);
+            }
+        }
+    } else {  // one destination per source vector
+        const long long total = copy_pairs<MODE>(a) * nvec;
+        for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += step) {
+            const long long i = w / nvec, j = w - (w / nvec) * nvec;
+            st_stream(copy_dst<MODE>(a, i, 0) + j * 16, ld_stream(copy_src<MODE>(a, i) + j * 16));
         }
     }
 }
@@ -631,13 +650,16 @@ __global__ void __launch_bounds__(kThreads) k_copy_vec(CopyArgs a) {
 template <int MODE, typename U>
 __global__ void __launch_bounds__(kThreads) k_copy_scalar(CopyArgs a) {
     const long long nu = a.unit / (long long)sizeof(U);
-    const long long total = copy_pairs<MODE>(a) * nu;
+    const int G = copy_groups<MODE>(a);
+    const long long per = copy_pairs<MODE>(a) * nu, total = per * G;
     const long long step = (long long)gridDim.x * blockDim.x;
     for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += step) {
-        const long long i = w / nu, j = w - (w / nu) * nu;
+        const long long gi = G == 1 ? 0 : w / per, r = w - gi * per;
+        const long long i = r / nu, j = r - i * nu;
         const U v = *(const U*)(copy_src<MODE>(a, i) + j * sizeof(U));
         const int nd = copy_ndst<MODE>(a);
-        for (int d = 0; d < nd; d++) {
+        const int d0 = (int)(nd * gi / G), d1 = (int)(nd * (gi + 1) / G);
+        for (int d = d0; d < d1; d++) {
             char* q = copy_dst<MODE>(a, i, d);
             if (q) *(U*)(q + j * sizeof(U)) = v;
         }

@@ -532,3 +532,20 @@ def test_in_place_allreduce_on_the_step_engines(engine, variant, P):
             comm.allreduce(buf, buf, count, code)
             comm.synchronize()
             assert torch.equal(buf.view(torch.uint8), expect.view(torch.uint8))
+
+
+@pytest.mark.parametrize("coll,P,count", [
+    ("reduce_scatter", 1024, 8), ("reduce_scatter", 256, 4), ("allreduce", 512, 64), ("allreduce", 64, 32),
+    ("reduce", 1024, 16), ("allgather", 1024, 8), ("allgather", 300, 4), ("bcast", 512, 8), ("bcast", 1000, 12),
+])
+def test_small_calls_at_large_p(coll, P, count):
+    """Few output columns at large P: column tiles of 16 or 8 columns (16 or
+    32 row groups) for the sums, destination groups for allgather and
+    bcast; results exact."""
+    comm = make_comm(P, coll, list(bine.VARIANTS[coll])[0])
+    for dt in (np.int32, np.int64):
+        sc, _ = buffer_counts(coll, count, P)
+        x = np.random.default_rng(P + count).integers(-1000, 1001, (P, sc)).astype(dt)
+        out = run(comm, coll, x, count, 0)
+        rr = receiving_ranks(coll, P, 0)
+        assert np.array_equal(out[rr], expected(coll, x, P, count, 0)[rr])
