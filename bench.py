@@ -445,8 +445,8 @@ def run_batch_suite(args):
             cm.set_stream(stream)
 
     # Autotuned batched launch (tuning cached on disk with a checksum).
-    cache = os.path.join(ROOT, "gpurun_out", "batch_tuning.json") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) \
-        else os.path.join(ROOT, ".batch_tuning.json")
+    cache = os.path.join(args.out or os.path.join(ROOT, "bench_out"), "batch_tuning.json")
+    os.makedirs(os.path.dirname(cache), exist_ok=True)
     table = tuning.load(cache)
     sig = tuning.signature(items, torch.cuda.get_device_name(0))
     tune_ms = None
@@ -567,7 +567,7 @@ def run_sweep_suite(args):
     import bine_trees_fugaku_b200 as bine
 
     torch.cuda.set_device(0)
-    out_dir = args.out or os.path.join(ROOT, "gpurun_out")
+    out_dir = args.out or os.path.join(ROOT, "bench_out")
     os.makedirs(out_dir, exist_ok=True)
     path = os.path.join(out_dir, "sweep.jsonl")
     stream = torch.cuda.current_stream()
@@ -773,7 +773,7 @@ def run_links_suite(args):
     import bine_trees_fugaku_b200 as bine
 
     torch.cuda.set_device(0)
-    out_dir = args.out or os.path.join(ROOT, "gpurun_out")
+    out_dir = args.out or os.path.join(ROOT, "bench_out")
     os.makedirs(out_dir, exist_ok=True)
     path = os.path.join(out_dir, "links.jsonl")
     stream = torch.cuda.current_stream()
@@ -858,7 +858,7 @@ def run_picker_suite(args):
     from bine_trees_fugaku_b200 import picker as pk
 
     torch.cuda.set_device(0)
-    out_dir = args.out or os.path.join(ROOT, "gpurun_out")
+    out_dir = args.out or os.path.join(ROOT, "bench_out")
     os.makedirs(out_dir, exist_ok=True)
 
     def log(m):

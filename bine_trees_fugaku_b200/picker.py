@@ -15,7 +15,7 @@ None of them changes a result: they only change time.
   link's bytes, both generated by this engine (bench.py --suite picker).
 * Model: bine_mlp (3 x 256, GELU, bf16 weights, fp32 accumulation),
   trained on the GPU with the engine's own kernels.
-* Judge: exhaustive search (every valid arm measured).  Fallback: the
+* Evaluated against exhaustive search (every valid arm measured).  Fallback: the
   reference's fixed rule (fixed_rule below), used when no model is loaded
   or the model's pick is not valid for the call.
 * Picker.choose applies the model's best provable arm; Picker.tune times
