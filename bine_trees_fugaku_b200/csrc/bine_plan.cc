@@ -1857,45 +1857,21 @@ bool split_trees(const TreePlan& tp, int K, SplitTrees* out, std::string* err) {
 namespace bine {
 namespace {
 
-// Element ranges of one row: start -> span.  Spans cover what some item has
-// touched; untouched gaps have no writer and no readers.
+// State of one row (buffer, rank) between levels: sorted, disjoint element
+// ranges with their last writer and the readers since.  Untouched gaps have
+// no writer and no readers.
 struct FlowSpan {
-    int64_t end;
-    int32_t writer;                // last item that wrote the span, -1: none
-    std::vector<int32_t> readers;  // items that read it since (ascending)
+    int64_t s, e;
+    int32_t writer;                // last item that wrote the range, -1: none
+    std::vector<int32_t> readers;  // items that read it since
 };
-using FlowRow = std::map<int64_t, FlowSpan>;
 
-// Splits the span containing x (if x falls strictly inside one) at x.
-void flow_split(FlowRow& row, int64_t x) {
-    auto it = row.upper_bound(x);
-    if (it == row.begin()) return;
-    --it;
-    if (it->first < x && x < it->second.end) {
-        FlowSpan right = it->second;
-        it->second.end = x;
-        row.emplace(x, std::move(right));
-    }
-}
-
-// Makes [s, e) a sequence of spans (gaps filled with untouched spans) and
-// calls f on each.
-template <typename F>
-void flow_cover(FlowRow& row, int64_t s, int64_t e, F f) {
-    flow_split(row, s);
-    flow_split(row, e);
-    int64_t pos = s;
-    auto it = row.lower_bound(s);
-    while (pos < e) {
-        if (it == row.end() || it->first > pos) {
-            const int64_t gap_end = it == row.end() ? e : std::min(e, it->first);
-            it = row.emplace_hint(it, pos, FlowSpan{gap_end, -1, {}});
-        }
-        f(it->second);
-        pos = it->second.end;
-        ++it;
-    }
-}
+// One access of one level: elements [s, e) of row `row`.
+struct FlowAccess {
+    int64_t s, e;
+    int32_t item;
+    bool write;
+};
 
 }  // namespace
 
@@ -1909,7 +1885,9 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
     max_item_elems = std::max(min_item_elems, max_item_elems);
     // Pieces and items, level by level.
     std::vector<const Move*> move_of;  // level-order move index -> move
+    std::vector<int32_t> level_first;  // first item of each level
     for (size_t l = 0; l < s.levels.size(); l++) {
+        level_first.push_back((int32_t)out->items.size());
         int64_t level_elems = 0;
         for (const Move& m : s.levels[l]) level_elems += m.n;
         int64_t item_elems = std::max(min_item_elems, (level_elems + target_items - 1) / target_items);
@@ -1942,59 +1920,119 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
         }
         out->level_items.push_back(nitems);
     }
-    // Dependencies over rows (buffer, rank).
-    auto row_id = [&](const Region& r) { return (size_t)r.buf * P + r.rank; };
-    std::vector<FlowRow> rows(kNumBufs * (size_t)P);
-    std::vector<int32_t> cand;
-    for (int32_t i = 0; i < (int32_t)out->items.size(); i++) {
-        FlowItem& it = out->items[i];
-        cand.clear();
-        // Reads first: read after write on the last writers; the item
-        // becomes a reader.
-        for (int32_t p = it.pbeg; p < it.pend; p++) {
-            const FlowPiece& pc = out->pieces[p];
-            const Move& m = *move_of[pc.move];
-            for (int k = 0; k < 1 + m.add; k++) {
-                const Region& r = k ? m.b : m.a;
-                flow_cover(rows[row_id(r)], r.off + pc.start, r.off + pc.start + pc.n, [&](FlowSpan& sp) {
-                    if (sp.writer >= 0) cand.push_back(sp.writer);
-                    if (sp.readers.empty() || sp.readers.back() != i) sp.readers.push_back(i);
-                });
+    level_first.push_back((int32_t)out->items.size());
+    // Dependencies, one level at a time: every access of the level is
+    // checked against the state its rows had before the level (moves of one
+    // level are independent), then each touched row's state is rebuilt in
+    // one sweep.  Rows are (buffer, rank).
+    const size_t nrows = kNumBufs * (size_t)P;
+    std::vector<std::vector<FlowSpan>> rows(nrows);
+    std::vector<std::vector<FlowAccess>> acc(nrows);
+    std::vector<size_t> touched;
+    std::vector<std::vector<int32_t>> cand;
+    std::vector<int64_t> bounds, abounds, obounds;
+    std::vector<FlowSpan> next;
+    for (size_t l = 0; l + 1 < level_first.size(); l++) {
+        const int32_t i0 = level_first[l], i1 = level_first[l + 1];
+        if (i0 == i1) continue;
+        touched.clear();
+        auto add = [&](const Region& r, int64_t st, int64_t n, int32_t item, bool write) {
+            const size_t row = (size_t)r.buf * P + r.rank;
+            if (acc[row].empty()) touched.push_back(row);
+            acc[row].push_back(FlowAccess{r.off + st, r.off + st + n, item, write});
+        };
+        for (int32_t i = i0; i < i1; i++)
+            for (int32_t p = out->items[i].pbeg; p < out->items[i].pend; p++) {
+                const FlowPiece& pc = out->pieces[p];
+                const Move& m = *move_of[pc.move];
+                add(m.a, pc.start, pc.n, i, false);
+                if (m.add) add(m.b, pc.start, pc.n, i, false);
+                add(m.dst, pc.start, pc.n, i, true);
             }
-        }
-        // Then writes: write after write on the last writer, write after
-        // read on the readers since; the item becomes the writer.
-        for (int32_t p = it.pbeg; p < it.pend; p++) {
-            const FlowPiece& pc = out->pieces[p];
-            const Move& m = *move_of[pc.move];
-            FlowRow& row = rows[row_id(m.dst)];
-            const int64_t s0 = m.dst.off + pc.start, s1 = s0 + pc.n;
-            flow_cover(row, s0, s1, [&](FlowSpan& sp) {
-                if (sp.writer >= 0) cand.push_back(sp.writer);
-                cand.insert(cand.end(), sp.readers.begin(), sp.readers.end());
-            });
-            row.erase(row.lower_bound(s0), row.lower_bound(s1));
-            row.emplace(s0, FlowSpan{s1, i, {}});
+        cand.assign(i1 - i0, {});
+        for (size_t row : touched) {
+            std::vector<FlowAccess>& A = acc[row];
+            std::vector<FlowSpan>& old = rows[row];
+            std::sort(A.begin(), A.end(), [](const FlowAccess& x, const FlowAccess& y) { return x.s < y.s; });
+            // Read after write on the last writers; write after write and
+            // write after read on the last writer and its readers.
+            for (const FlowAccess& a : A) {
+                auto it = std::upper_bound(old.begin(), old.end(), a.s,
+                                           [](int64_t v, const FlowSpan& sp) { return v < sp.e; });
+                std::vector<int32_t>& c = cand[a.item - i0];
+                for (; it != old.end() && it->s < a.e; ++it) {
+                    if (it->writer >= 0) c.push_back(it->writer);
+                    if (a.write) c.insert(c.end(), it->readers.begin(), it->readers.end());
+                }
+            }
+            // New state: the elementary ranges between all boundaries; a
+            // range written this level belongs to its writer alone, others
+            // keep their writer and add this level's readers.
+            // The old spans' boundaries are already in order: sort only the
+            // accesses' and merge.
+            abounds.clear();
+            for (const FlowAccess& a : A) abounds.push_back(a.s), abounds.push_back(a.e);
+            std::sort(abounds.begin(), abounds.end());
+            obounds.clear();
+            for (const FlowSpan& sp : old) obounds.push_back(sp.s), obounds.push_back(sp.e);
+            bounds.resize(abounds.size() + obounds.size());
+            std::merge(obounds.begin(), obounds.end(), abounds.begin(), abounds.end(), bounds.begin());
+            bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
+            next.clear();
+            size_t oi = 0, ai = 0;
+            std::vector<const FlowAccess*> live;  // accesses covering the current range
+            for (size_t b = 0; b + 1 < bounds.size(); b++) {
+                const int64_t x0 = bounds[b], x1 = bounds[b + 1];
+                while (oi < old.size() && old[oi].e <= x0) oi++;
+                const FlowSpan* os = oi < old.size() && old[oi].s <= x0 ? &old[oi] : nullptr;
+                while (ai < A.size() && A[ai].s <= x0) live.push_back(&A[ai++]);
+                live.erase(std::remove_if(live.begin(), live.end(), [&](const FlowAccess* a) { return a->e <= x0; }),
+                           live.end());
+                if (!os && live.empty()) continue;  // a gap nobody touches
+                FlowSpan sp{x0, x1, os ? os->writer : -1, {}};
+                const FlowAccess* w = nullptr;
+                for (const FlowAccess* a : live)
+                    if (a->write) w = a;
+                if (w) {
+                    sp.writer = w->item;
+                } else {
+                    if (os) sp.readers = os->readers;
+                    for (const FlowAccess* a : live)
+                        if (std::find(sp.readers.begin(), sp.readers.end(), a->item) == sp.readers.end())
+                            sp.readers.push_back(a->item);
+                }
+                if (!next.empty() && next.back().e == x0 && next.back().writer == sp.writer &&
+                    next.back().readers == sp.readers)
+                    next.back().e = x1;
+                else
+                    next.push_back(std::move(sp));
+            }
+            old.swap(next);
+            A.clear();
         }
         // Earlier levels only, one entry per item, and a level entry where
         // one level would contribute more than kFlowLevelDep items.
-        std::sort(cand.begin(), cand.end());
-        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-        it.dbeg = (int32_t)out->deps.size();
-        size_t j = 0;
-        while (j < cand.size()) {
-            const int32_t lv = out->items[cand[j]].level;
-            size_t k = j;
-            while (k < cand.size() && out->items[cand[k]].level == lv) k++;
-            if (lv < it.level) {
-                if (k - j > (size_t)kFlowLevelDep)
-                    out->deps.push_back(-(lv + 1));
-                else
-                    out->deps.insert(out->deps.end(), cand.begin() + j, cand.begin() + k);
+        for (int32_t i = i0; i < i1; i++) {
+            std::vector<int32_t>& c = cand[i - i0];
+            std::sort(c.begin(), c.end());
+            c.erase(std::unique(c.begin(), c.end()), c.end());
+            FlowItem& it = out->items[i];
+            it.dbeg = (int32_t)out->deps.size();
+            size_t j = 0;
+            while (j < c.size()) {
+                const int32_t lv = out->items[c[j]].level;
+                size_t k = j;
+                while (k < c.size() && out->items[c[k]].level == lv) k++;
+                if (lv < it.level) {
+                    if (k - j > (size_t)kFlowLevelDep)
+                        out->deps.push_back(-(lv + 1));
+                    else
+                        out->deps.insert(out->deps.end(), c.begin() + j, c.begin() + k);
+                }
+                j = k;
             }
-            j = k;
+            it.dend = (int32_t)out->deps.size();
         }
-        it.dend = (int32_t)out->deps.size();
     }
 }
 

@@ -171,10 +171,10 @@ class Planner {
 // `min_item_elems` unless the level is smaller).  With piece_elems <= 0 the
 // pieces take the item size of their level, rounded up to a multiple of
 // `min_item_elems` and capped at `max_item_elems`.  Each item lists the
-// earlier items it must wait for over every (buffer, rank) row: the last
-// writer of what it reads (read after write) and of what it writes (write
-// after write), and every reader since that writer of what it writes (write
-// after read).  A dependency is an item index >= 0, or -(l + 1) for "every
+// earlier items it must wait for over every (buffer, rank) row, as the row
+// stood before the item's level: the last writer of what it reads (read
+// after write) and of what it writes (write after write), and every reader
+// since that writer of what it writes (write after read).  A dependency is an item index >= 0, or -(l + 1) for "every
 // item of level l", used where one level would contribute more than
 // kFlowLevelDep items.  Items are in level order and every dependency is on
 // an earlier level, so running items in index order, each after its
