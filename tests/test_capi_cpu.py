@@ -87,3 +87,20 @@ def test_collective_argument_errors_are_reported_before_any_device_work():
         c.set_host_window(100)
     with err(None):
         c.set_segment(-5)
+
+
+def test_hooked_host_allreduce_argument_errors_and_zero_count():
+    """bine_allreduce_host_hooked rejects a null communicator and any op but
+    SUM before touching the device; with count 0 it succeeds without calling
+    either hook."""
+    L = bine.lib()
+    z = np.zeros((8, 1), np.int32)
+    null_hook = bine.WINDOW_HOOK()
+    assert L.bine_allreduce_host_hooked(z.ctypes.data, z.ctypes.data, 1, bine.INT32, bine.SUM, None,
+                                        null_hook, null_hook, None) == bine.ERR_ARG
+    c = bine.Comm(8)
+    with pytest.raises(bine.BineError, match="bine error 1:"):
+        c.allreduce_host_hooked(z, z, 1, bine.INT32, op=1)
+    calls = []
+    c.allreduce_host_hooked(z, z, 0, bine.INT32, before=lambda f, n: calls.append(f), after=lambda f, n: calls.append(f))
+    assert calls == []
