@@ -1095,6 +1095,16 @@ void row_elems(int coll, long long count, int P, long long* se, long long* re) {
     }
 }
 
+// Whether the rank-major arrays [a, a + ast*(P-1) + arow) and
+// [b, b + bst*(P-1) + brow) share any byte.
+bool arrays_overlap(const void* a, long long ast, size_t arow, const void* b, long long bst, size_t brow, int P) {
+    if (!a || !b || !arow || !brow) return false;
+    const uintptr_t a0 = (uintptr_t)a, b0 = (uintptr_t)b;
+    const uintptr_t a1 = a0 + (uintptr_t)ast * (uintptr_t)(P - 1) + arow;
+    const uintptr_t b1 = b0 + (uintptr_t)bst * (uintptr_t)(P - 1) + brow;
+    return a0 < b1 && b0 < a1;
+}
+
 int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, long long count, int dt, int root) {
     if (!c) return fail(BINE_ERR_ARG, "null communicator");
     const int es = dtype_size(dt);
@@ -1114,14 +1124,18 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
     char* out = (char*)recvbuf;
     PlanKey k = make_key(c, coll, count, root);
 
-    // In place (MPI_IN_PLACE): the step schedules read a rank's send row in
-    // the same step that writes receive rows (the L butterfly reads its
-    // peer's input while the peer's result is written), which is a race
-    // once the two rows are one.  The step engines therefore take the input
-    // rows from a staged copy; the fused kernels read every input of a tile
-    // before writing it and need none.
-    if ((c->engine == BINE_ENGINE_STEPS || c->engine == BINE_ENGINE_PIPELINED) && coll == kAllreduce &&
-        (const void*)in == (const void*)out) {
+    // Input and output arrays that share bytes (MPI_IN_PLACE, or rows laid
+    // out so that they interleave): the step schedules read a rank's send
+    // row in the same step that writes receive rows (the L butterfly reads
+    // its peer's input while the peer's result is written), and the copy
+    // kernels and the reduce_scatter tiles write rows that other blocks still
+    // read.  Such calls take their input rows from a staged copy.  The one
+    // exception is an allreduce or reduce on the FUSED engine whose arrays
+    // are one (same base, same stride): every tile reads its columns of all
+    // rows before writing the same columns, and no other tile touches them.
+    if (arrays_overlap(in, ist, (size_t)se * es, out, ost, (size_t)re * es, c->P) &&
+        !(c->engine == BINE_ENGINE_FUSED && (coll == kAllreduce || coll == kReduce) &&
+          (const void*)in == (const void*)out && ist == ost)) {
         const size_t pitch = ((size_t)se * es + 255) / 256 * 256, bytes = pitch * (size_t)c->P;
         if (c->inplace_bytes < bytes) {
             CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1427,9 +1441,11 @@ int noalloc_run(bine_comm_t c, const Schedule& s, const char* send, long long is
     const size_t off_lb = 256, off_mv = off_lb + round256(lb.size() * sizeof(int));
     const size_t off_ch = off_mv + round256(moves.size() * sizeof(dev::StepMove));
     const size_t off_ws = off_ch + round256(chunks.size() * sizeof(dev::StepChunk));
-    // In place: the input rows are staged after the workspace (the step
-    // schedule would otherwise read rows the same step overwrites).
-    const bool in_place = (const void*)send == (const void*)recv;
+    // Input and output arrays that share bytes: the input rows are staged
+    // after the workspace (the step schedule would otherwise read rows the
+    // same step overwrites).
+    const bool in_place = arrays_overlap(send, ist, (size_t)s.send_elems * sizeof(T), recv, ost,
+                                         (size_t)s.recv_elems * sizeof(T), c->P);
     const size_t in_pitch = round256((size_t)s.send_elems * sizeof(T));
     const size_t off_in = off_ws + tmp_stride * (size_t)c->P;
     const size_t need = off_in + (in_place ? in_pitch * (size_t)c->P : 0);
@@ -1474,7 +1490,7 @@ int noalloc_run(bine_comm_t c, const Schedule& s, const char* send, long long is
     unsigned* bar = (unsigned*)base;
     int* status = (int*)(base + 16);
     unsigned long long to = c->step_timeout_ns;
-    unsigned expected = (unsigned)blocks;
+    unsigned expected = (unsigned)blocks + c->barrier_extra;
     void* args[] = {&B, &mv, &ch, &lbp, &nl, &bar, &status, &to, &expected};
     CUDA_TRY(cudaLaunchCooperativeKernel((void*)dev::k_steps<T>, dim3(blocks), dim3(dev::kThreads), args, 0, st));
     // The host staging of the tables and the status check need the call to

@@ -5,8 +5,12 @@
  * one GPU.  Every buffer argument is a DEVICE pointer to a rank-major array:
  * rank r's row starts at  base + r * stride  bytes.  By default the stride is
  * the row size (rows packed back to back); bine_comm_set_layout() sets a
- * larger one.  Calls are asynchronous and ordered on the communicator's CUDA
- * stream.  Functions return BINE_SUCCESS or an error code and never abort;
+ * larger one.  Input and output arrays may share bytes (the same base, as
+ * with MPI_IN_PLACE, or rows that interleave): such a call first copies its
+ * input rows to a staging area of the communicator, except an allreduce or
+ * reduce on the FUSED engine whose two arrays are identical (same base and
+ * stride), which needs no copy.  Calls are asynchronous and ordered on the
+ * communicator's CUDA stream.  Functions return BINE_SUCCESS or an error code and never abort;
  * bine_last_error_string() describes the last error of the calling thread.
  *
  * The eight collectives keep the argument lists of the reference library's

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference at REF (default /root/reference)
-and the reference library built by `make -C oracle ref`:
+Run in a checkout that has the reference at REF (default: $BINE_REFERENCE,
+else a directory "reference" beside this repository) and the reference
+library built by `make -C oracle ref`:
 
     python tests/golden/make_golden.py [REF]
 
@@ -91,7 +92,9 @@ def ref_collectives():
 
 
 def main():
-    refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    repo = os.path.dirname(os.path.dirname(HERE))
+    refdir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+        "BINE_REFERENCE", os.path.join(os.path.dirname(repo), "reference"))
     if not ref.available():
         sys.exit("build the reference first: make -C oracle ref")
     with open(os.path.join(HERE, "remap_rank.json"), "w") as f:

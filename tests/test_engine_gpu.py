@@ -549,3 +549,35 @@ def test_small_calls_at_large_p(coll, P, count):
         out = run(comm, coll, x, count, 0)
         rr = receiving_ranks(coll, P, 0)
         assert np.array_equal(out[rr], expected(coll, x, P, count, 0)[rr])
+
+
+@pytest.mark.parametrize("engine", ["fused", "steps", "pipelined"])
+@pytest.mark.parametrize("coll", ["allreduce", "reduce_scatter", "reduce", "allgather", "alltoall", "scatter", "gather"])
+@pytest.mark.parametrize("layout", ["same_base", "offset_rows"])
+def test_overlapping_arrays_match_separate_arrays(engine, coll, layout):
+    """Input and output arrays that share bytes: the same base address with
+    each array's own packed rows (MPI_IN_PLACE-like), or output rows that
+    start one input row further on.  Such calls stage their input rows first
+    (except an allreduce or reduce on the FUSED engine whose arrays are one),
+    so every engine gives the bytes of separate arrays, float32 included."""
+    P = 16
+    count = P * 37 + 5 if coll == "allreduce" else 37
+    sc, rc = buffer_counts(coll, count, P)
+    variant = list(bine.VARIANTS[coll])[0]
+    comm = make_comm(P, coll, variant, engine=engine)
+    rr = receiving_ranks(coll, P, 0)
+    for dt, code in ((np.int32, bine.INT32), (np.float32, bine.FLOAT)):
+        rng = np.random.default_rng(P + sc)
+        x = (rng.integers(-1000, 1001, (P, sc)) if dt == np.int32 else rng.standard_normal((P, sc))).astype(dt)
+        want = run(comm, coll, x, count)
+        shift = 0 if layout == "same_base" else sc
+        tdt = torch.int32 if dt == np.int32 else torch.float32
+        flat = torch.zeros(shift + P * max(sc, rc), dtype=tdt, device="cuda")
+        for _ in range(2):
+            flat.zero_()
+            flat[:P * sc] = torch.from_numpy(x.ravel()).cuda()
+            send, recv = flat[:P * sc], flat[shift:shift + P * rc]
+            comm.run(coll, send, recv, count, code, 0)
+            comm.synchronize()
+            got = recv.view(P, rc).cpu().numpy()
+            assert np.array_equal(got[rr].view(np.uint32), want[rr].view(np.uint32)), (dt, layout)

@@ -118,13 +118,14 @@ def test_reduce_scatter_volume_per_step_is_uniform_over_blocks(ports):
     count = P * ports * 3 + 5
     msgs = comm.plan_messages("allreduce", count)
     S = 6
-    for p in range(ports):
-        pass
+    # Port p reduces its own slice of count_p elements (lib/libbine.cc:986-1010).
+    per_port = [count // ports + (p < count % ports) for p in range(ports)]
     for i in range(S):
         lvl = msgs[msgs[:, 0] == i + 1]
-        assert int(lvl[:, 3].sum()) == (P * count) >> (i + 1) or ports > 1
+        # Each of a port's blocks leaves P / 2^(i+1) ranks at step i.
+        assert int(lvl[:, 3].sum()) == sum(c * (P >> (i + 1)) for c in per_port), i
     total_rs = sum(int(msgs[msgs[:, 0] == i + 1][:, 3].sum()) for i in range(S))
-    assert total_rs == sum((P * (count // ports + (p < count % ports))) * (2 ** S - 1) // 2 ** S for p in range(ports))
+    assert total_rs == sum(P * c * (2 ** S - 1) // 2 ** S for c in per_port)
 
 
 @pytest.mark.parametrize("case", [c for c in CASES if c["ok"]], ids=lambda c: f"{c['coll']}-{c['variant']}-P{c['P']}"

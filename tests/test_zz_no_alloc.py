@@ -90,3 +90,25 @@ def test_noalloc_in_place_matches_out_of_place():
         assert noalloc_allreduce(comm, buf, buf, count, bine.FLOAT) == bine.SUCCESS, bine.last_error()
         torch.cuda.synchronize()
         assert torch.equal(buf, want)
+
+
+def test_noalloc_barrier_timeout_is_reported_and_recoverable():
+    """A grid barrier told to wait for one arrival that never comes (fault
+    injected on the host) expires after the configured bound: the call
+    reports BINE_ERR_TIMEOUT, and the next call on the same scratch is
+    correct.  The wait is bounded, so nothing hangs."""
+    P, count = 16, 16 * 64
+    comm = bine.Comm(P)
+    comm.set_algo("allreduce", "B")
+    comm.set_stream(torch.cuda.current_stream())
+    x = np.random.default_rng(6).integers(-1000, 1001, (P, count)).astype(np.int32)
+    send = torch.from_numpy(x).cuda()
+    recv = torch.zeros_like(send)
+    comm.set_step_timeout(200)
+    comm.debug_set_barrier_extra(1)
+    assert noalloc_allreduce(comm, send, recv, count, bine.INT32) == bine.ERR_TIMEOUT
+    assert "timed out" in bine.last_error()
+    comm.debug_set_barrier_extra(0)
+    assert noalloc_allreduce(comm, send, recv, count, bine.INT32) == bine.SUCCESS, bine.last_error()
+    want = x.astype(np.int64).sum(0).astype(np.int32)
+    assert np.array_equal(recv.cpu().numpy(), np.broadcast_to(want, (P, count)))
