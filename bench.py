@@ -150,10 +150,12 @@ def reference_time(steps, warmup, budget_s=150.0):
         return {"error": "reference run failed", "detail": j}
     t = j["median_s"]
     gbs = 2 * P_RANKS * count * ES / t / 1e9
+    cores = os.cpu_count()
     sample = (f"P={P_RANKS} allreduce, {count} int32 per rank ({'full workload' if count == COUNT else 'scaled sample'}), "
               f"{steps} timed calls after {warmup} warm-ups; per call: two barriers, wall time around one call, "
-              f"max over ranks, median over calls (bench/bench.cc:289-318, 376-387)")
-    return {"value": gbs, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference", "sample": sample,
+              f"max over ranks, median over calls (bench/bench.cc:289-318, 376-387); {P_RANKS} processes on "
+              f"{cores} cores" + (" (oversubscribed: more ranks than cores)" if P_RANKS > cores else ""))
+    return {"value": gbs, "unit": "GB/s", "cores": cores, "kind": "reference", "sample": sample,
             "median_s": t, "count": count}
 
 
@@ -244,23 +246,36 @@ def run_engine_arm(args):
     comm.synchronize()
     # Correctness of the timed configuration: exact integer sums; float
     # sums within 1e-4 relative of FP64 (checked bit for bit by the tests).
+    # Every rank's row is checked.
     if args.dtype == "int32":
         expect = send.sum(0, dtype=torch.int64).to(torch.int32)
-        ok = bool(torch.equal(recv[0], expect) and torch.equal(recv[-1], expect))
+        ok = bool((recv == expect).all())
     else:
-        expect = send.double().sum(0)
-        ok = bool(torch.allclose(recv[0].double(), expect, rtol=1e-4, atol=1e-4) and torch.equal(recv[0], recv[-1]))
+        s64 = send.double().sum(0)
+        floor = send.abs().double().sum(0) * (P_RANKS * 2.0 ** -24)
+        ok = bool(((recv[0].double() - s64).abs() <= floor + 1e-30).all() and (recv == recv[0]).all())
         expect = recv[0].clone()
 
+    # The timed region: exactly K steps between a barrier + synchronize on
+    # both sides.  It is repeated until the repeats span at least a second,
+    # so that the clock sampler (100 ms period) sees it; the line reports
+    # the median repeat (each the max over ranks).
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    repeats, reps_ms = 1, []
     with ClockSampler(local) as clocks:
-        barrier()
-        start.record(stream)
-        for _ in range(args.steps):
-            step()
-        end.record(stream)
-        barrier()
-    elapsed_ms = max_over_ranks(start.elapsed_time(end), dist, "cuda")
+        while True:
+            barrier()
+            start.record(stream)
+            for _ in range(args.steps):
+                step()
+            end.record(stream)
+            barrier()
+            reps_ms.append(max_over_ranks(start.elapsed_time(end), dist, "cuda"))
+            # Every rank takes the same decision (from the max over ranks).
+            if len(reps_ms) >= 200 or sum(reps_ms) >= 1000.0:
+                break
+        repeats = len(reps_ms)
+    elapsed_ms = statistics.median(reps_ms)
     ms_per_step = elapsed_ms / args.steps
     value = world * ALGO_BYTES / (ms_per_step * 1e-3) / 1e9
     per_launch_gbs = ALGO_BYTES / (ms_per_step * 1e-3) / 1e9
@@ -304,6 +319,9 @@ def run_engine_arm(args):
                        "l2": "inputs 1 GiB and outputs 1 GiB exceed the 126 MB L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": per_launch_gbs, "peak": peak, "unit": "GB/s",
                          "frac": per_launch_gbs / peak, "traffic": profiled_traffic(),
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch from the "
+                                           "committed ncu capture (" + os.path.relpath(PROFILE_SUMMARY, ROOT) +
+                                           "), not measured in this run",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "algorithmic_bytes_per_launch": ALGO_BYTES},
             "cpu_baseline": cpu,
@@ -313,6 +331,10 @@ def run_engine_arm(args):
                 "path": "Comm.allreduce_host (C ABI bine_allreduce_host) with pinned host buffers; every step "
                         "copies all inputs to the GPU and every rank's result back, in pipelined column windows"},
             "gpu_launches": args.steps,
+            "timed_repeats": {"repeats": repeats, "ms_per_repeat_median": elapsed_ms,
+                              "ms_per_repeat_min": min(reps_ms), "ms_per_repeat_max": max(reps_ms),
+                              "note": "the K-step timed region repeated until the repeats span >= 1 s; "
+                                      "gpu_launches counts one repeat"},
             "clocks": clocks.summary(),
             "correct": ok,
         }
@@ -519,13 +541,17 @@ def sweep_algo_bytes(coll, P, count, es):
     return 2 * P * P * count * es  # alltoall
 
 
-def sweep_check(coll, send, recv, P, count, is_float, chunk_elems=1 << 25):
-    """MPI-semantics check of one sweep point, in column chunks so that the
-    temporaries stay small: integers and copies exactly, float sums within
-    1e-5 of sum|x| of an FP64 sum."""
+def sweep_check(coll, send, recv, P, count, is_float, order=None, chunk_elems=1 << 25, ref_cache=None):
+    """Check of one sweep point, in column chunks so that the temporaries
+    stay small: integers and copies exactly against MPI semantics; float32
+    sums in the FAST order within 1e-6 relative of an FP64 sum (plus the
+    FP64 sum's own uncertainty, P * 2^-52 * sum|x|); float32 sums in the
+    reference's order bit for bit against the oracle (ref_order_check)."""
     import torch
 
     if coll in ("allreduce", "reduce_scatter"):
+        if is_float and order == "reference":
+            return ref_order_check(coll, send, recv, P, count, ref_cache)
         n = send.shape[1]
         flat = recv.reshape(-1) if coll == "reduce_scatter" else None
         step = max(1, chunk_elems // P)
@@ -535,8 +561,8 @@ def sweep_check(coll, send, recv, P, count, is_float, chunk_elems=1 << 25):
             got = recv[:, a:b] if coll == "allreduce" else flat[a:b].unsqueeze(0)
             if is_float:
                 ssum = blk.sum(0, dtype=torch.float64)
-                scale = blk.abs().sum(0, dtype=torch.float64)
-                if not bool(((got.double() - ssum).abs() <= 1e-5 * scale + 1e-30).all()):
+                floor = blk.abs().sum(0, dtype=torch.float64) * (P * 2.0 ** -52)
+                if not bool(((got.double() - ssum).abs() <= 1e-6 * ssum.abs() + floor).all()):
                     return False
             elif not bool((got == blk.sum(0)).all()):
                 return False
@@ -549,6 +575,68 @@ def sweep_check(coll, send, recv, P, count, is_float, chunk_elems=1 << 25):
         return bool((recv == recv[0:1]).all())
     # alltoall: recv[q, r*count + j] = send[r, q*count + j]
     return all(bool(torch.equal(recv[:, r * count:(r + 1) * count], send[r].view(P, count))) for r in range(P))
+
+
+REF_ORDER_FULL_BYTES = 64 << 20
+
+
+def ref_order_columns(coll, P, count):
+    """Send-row columns whose results are checked against the oracle, and
+    the count of the oracle's call.  Small inputs are checked whole.  Larger
+    ones are checked on four columns of every block (first, second, middle,
+    last): the reference's addition tree of an element depends only on the
+    block it lies in, not on the block's length, so an oracle call with four
+    columns per block evaluates the same trees.  Blocks: allreduce splits
+    the count into P blocks, the remainder going to the first ones
+    (lib/libbine.cc:971-1010); reduce_scatter's block b is columns
+    [b*count, (b+1)*count) of every send row."""
+    import numpy as np
+
+    if P * count * 4 * (P if coll == "reduce_scatter" else 1) <= REF_ORDER_FULL_BYTES:
+        return None, count
+    if coll == "allreduce":
+        sizes = np.array([count // P + (b < count % P) for b in range(P)], np.int64)
+    else:
+        sizes = np.full(P, count, np.int64)
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    pos = np.stack([np.zeros(P, np.int64), np.minimum(1, sizes - 1), sizes // 2, sizes - 1], 1)
+    cols = (offs[:, None] + pos).reshape(-1)
+    return cols, (4 * P if coll == "allreduce" else 4)
+
+
+def ref_order_check(coll, send, recv, P, count, cache=None):
+    """Float32 results in the reference's order against the oracle (the
+    C++ restatement of the reference's MPI layer, variant B / contiguous
+    reduce_scatter, one port, a ring of P), bit for bit.  The oracle is the
+    checker here, run outside the timed region; `cache` keeps its result for
+    the other engines of the same point."""
+    import numpy as np
+    import torch
+
+    from oracle import port
+
+    key = (coll, P, count)
+    if cache is not None and key in cache:
+        cols, want = cache[key]
+    else:
+        cols, n = ref_order_columns(coll, P, count)
+        x = send if cols is None else send[:, torch.from_numpy(cols).to(send.device)]
+        want, _ = port.run(coll, x.cpu().numpy(), n, variant="B" if coll == "allreduce" else None)
+        if cache is not None:
+            cache.clear()
+            cache[key] = (cols, want)
+    if coll == "allreduce":
+        got = recv if cols is None else recv[:, torch.from_numpy(cols).to(recv.device)]
+        got = got.cpu().numpy()
+    else:
+        if cols is None:
+            got = recv.cpu().numpy()
+        else:
+            b = np.repeat(np.arange(P), 4)
+            j = cols - b * count
+            got = recv[torch.from_numpy(b).to(recv.device), torch.from_numpy(j).to(recv.device)].cpu().numpy()
+            got = got.reshape(P, 4)
+    return bool(np.array_equal(got.view(np.uint32), want.view(np.uint32)))
 
 
 def run_sweep_suite(args):
@@ -574,6 +662,11 @@ def run_sweep_suite(args):
     dtypes = [("float32", torch.float32, bine.FLOAT, 4), ("int64", torch.int64, bine.INT64, 8)]
     g = torch.Generator(device="cuda")
     rows, skipped, bad = [], [], []
+    ref_cache = {}
+
+    # A 256 MiB buffer written before every timed call evicts the 126 MB
+    # L2, so each call starts cold, as a call on fresh data would.
+    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def time_call(comm, coll, send, recv, count, code):
         comm.run(coll, send, recv, count, code)
@@ -584,14 +677,16 @@ def run_sweep_suite(args):
         e1.record(stream)
         e1.synchronize()
         one = max(e0.elapsed_time(e1), 1e-3)
-        reps = int(min(100, max(3, 20.0 / one)))
-        e0.record(stream)
-        for _ in range(reps):
+        reps = int(min(50, max(3, 10.0 / one)))
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for a, b in evs:
+            l2_flush.fill_(1)
+            a.record(stream)
             comm.run(coll, send, recv, count, code)
-        e1.record(stream)
-        e1.synchronize()
+            b.record(stream)
+        evs[-1][1].synchronize()
         comm.synchronize()
-        return e0.elapsed_time(e1) / reps * 1e3  # microseconds
+        return statistics.median(a.elapsed_time(b) for a, b in evs) * 1e3  # microseconds
 
     t_start = time.time()
     with open(path, "w") as f:
@@ -645,7 +740,8 @@ def run_sweep_suite(args):
                             except bine.BineError as e:
                                 emit(dict(point, engine=engine, unsupported=str(e)[:160]))
                                 continue
-                            ok = sweep_check(coll, send, recv, P, count, dname == "float32")
+                            ok = sweep_check(coll, send, recv, P, count, dname == "float32", order,
+                                             ref_cache=ref_cache)
                             ab = sweep_algo_bytes(coll, P, count, es)
                             r = dict(point, engine=engine, float_order=order if dname == "float32" else None,
                                      us=t_us, algo_gbs=ab / (t_us * 1e-6) / 1e9, correct=ok)
@@ -703,7 +799,11 @@ def run_sweep_suite(args):
         if eng == "steps" and (coll, P, nb, dt, "pipelined") in us:
             band = "below 64 KiB" if nb < 65536 else ("64 KiB to 2 MiB" if nb < 2 << 20 else "2 MiB and up")
             ratio.setdefault(band, []).append(t / us[(coll, P, nb, dt, "pipelined")])
+    sums = [r for r in timed if r["dtype"] == "float32" and r["coll"] in ("allreduce", "reduce_scatter")]
     line = {"suite": "sweep", "points_timed": len(timed), "points_incorrect": len(bad),
+            "float_sums_bit_exact_vs_oracle": len([r for r in sums if r["float_order"] == "reference" and r["correct"]]),
+            "float_sums_fast_within_1e-6_of_fp64": len([r for r in sums if r["float_order"] == "fast" and r["correct"]]),
+            "timing": "median of per-call CUDA-event times, L2 flushed (256 MiB written) before every call",
             "steps_over_pipelined_time_geomean": {k: round(float(np.exp(np.mean(np.log(v)))), 3)
                                                   for k, v in sorted(ratio.items())},
             "reference_points": len([r for r in refs if "speedup" in r]),

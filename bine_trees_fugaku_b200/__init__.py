@@ -211,6 +211,12 @@ class Comm:
         self._h = h
         self.nranks = nranks
         self.dims = dims or [nranks]
+        # Settings as last set (the picker reads them): per-collective
+        # variant (None: the reference's default), ports, engine, float order.
+        self.algo = {}
+        self.ports = 1
+        self.engine = "fused"
+        self.float_order = "reference"
 
     def close(self):
         if getattr(self, "_h", None):
@@ -234,20 +240,24 @@ class Comm:
 
     def set_ports(self, ports):
         check(lib().bine_comm_set_ports(self._h, ports))
+        self.ports = ports
 
     def set_algo(self, coll, variant, family="BINE", distance=None):
         check(lib().bine_comm_set_algo(self._h, COLL_ID[coll], VARIANTS[coll][variant], FAMILY[family],
                                        DISTANCE[distance]))
+        self.algo[coll] = variant
 
     def set_engine(self, engine):
         check(lib().bine_comm_set_engine(self._h, {"fused": ENGINE_FUSED, "steps": ENGINE_STEPS,
                                                              "pipelined": ENGINE_PIPELINED}.get(engine, engine)))
+        self.engine = {ENGINE_FUSED: "fused", ENGINE_STEPS: "steps", ENGINE_PIPELINED: "pipelined"}.get(engine, engine)
 
     def set_segment(self, segment_bytes):
         check(lib().bine_comm_set_segment(self._h, segment_bytes))
 
     def set_float_order(self, order):
         check(lib().bine_comm_set_float_order(self._h, {"reference": ORDER_REFERENCE, "fast": ORDER_FAST}.get(order, order)))
+        self.float_order = {ORDER_REFERENCE: "reference", ORDER_FAST: "fast"}.get(order, order)
 
     def set_step_timeout(self, ms):
         check(lib().bine_comm_set_step_timeout(self._h, ms))

@@ -5,7 +5,16 @@ For each call it picks the schedule the STEPS engine runs: the Bine variant
 reduce-scatter + allgather "B", "B_COALESCE", "B_CONT"), the port count
 and the segment size (the engine's unit of work per block).  These are the
 choices the reference leaves to LIBBINE_* variables and its sweep scripts.
-None of them changes a result: they only change time.
+The picker never changes a result:
+
+* integer sums and copies are exact whatever the arm;
+* a float32 sum in the reference's order is a different addition tree for
+  every variant and port count (the port count splits the vector into
+  different blocks, lib/libbine.cc:986-1010), so for those calls the picker
+  keeps the caller's variant and port count and chooses the segment only,
+  which moves the same data in different units.  Only FAST-order float
+  calls on the FUSED engine, whose sums do not follow the schedule, are
+  free in every knob.
 
 * Features (one row per call): op one-hot, log2 P, log2 message bytes,
   torus shape (number of dimensions and log2 of each), dtype one-hot, and
@@ -149,6 +158,57 @@ def fixed_rule(coll, P, count, es):
             ports = 2 if ports == 6 else 1
         arm = ("allgather", v, ports, seg)
     return ARMS.index(arm)
+
+
+FLOAT_CODES = (2, 3)  # BINE_FLOAT, BINE_DOUBLE
+REDUCTIONS = ("allreduce", "reduce_scatter")
+DEFAULT_VARIANT = {"allreduce": "B", "reduce_scatter": "VEC_HALVING_CONT_PERMUTE",
+                   "allgather": "VEC_DOUBLING_CONT_PERMUTE"}
+
+
+def order_bound(coll, datatype, engine="steps", float_order="reference"):
+    """Whether the call's result bits depend on the variant and port count:
+    float sums in the reference's order (the STEPS and PIPELINED engines
+    always keep it; the FUSED engine unless set to FAST)."""
+    return coll in REDUCTIONS and datatype in FLOAT_CODES and not (engine == "fused" and float_order == "fast")
+
+
+def keep_of(comm, coll):
+    """The caller's (variant, ports) for `coll` on `comm`."""
+    return comm.algo.get(coll, DEFAULT_VARIANT[coll]), comm.ports
+
+
+def arm_keeps(arm, keep):
+    return keep is None or (arm[1], arm[2]) == tuple(keep)
+
+
+def fallback_arm(config, valid=None):
+    """The arm the fixed rule ends up running: its own pick, or, where the
+    engine refuses that (valid[a] False), the first valid latency-optimal
+    tree (allreduce) or block-by-block allgather, as Picker does without a
+    model; None when nothing runs."""
+    c = config
+    first = fixed_rule(c["coll"], c["P"], c["count"], c["es"])
+    if valid is None or valid[first]:
+        return first
+    for a, arm in enumerate(ARMS):
+        if valid[a] and arm[0] == c["coll"] and arm[1] in ("L", "VEC_DOUBLING_BLOCKS"):
+            return a
+    return None
+
+
+def allowed_arms(config, valid=None):
+    """Arm mask of a measured call for the evaluation: every arm for integer
+    calls; for float reductions (reference order) the arms with the variant
+    and port count the fixed rule runs (fallback_arm), i.e. the segment
+    choice alone."""
+    m = np.ones(NARMS, bool)
+    if config["coll"] in REDUCTIONS and config.get("dtype") == "float":
+        fa = fallback_arm(config, valid)
+        if fa is None:
+            return np.zeros(NARMS, bool)
+        m = np.array([arm_keeps(a, ARMS[fa][1:3]) for a in ARMS])
+    return m
 
 
 def apply_arm(comm, arm):
@@ -381,7 +441,9 @@ def evaluate(pred, T, Lb, valid, configs, shortlist=3):
     rows, within, ratio, speed, fixed_within, fixed_invalid = 0, 0, [], [], 0, 0
     link_exact, link_ratio, short_within = 0, [], 0
     for i in range(T.shape[0]):
-        v = valid[i]
+        # Float reductions: only arms that keep the reference order's
+        # variant and ports (the result bits) compete.
+        v = valid[i] & allowed_arms(configs[i], valid[i])
         if not v.any():
             continue
         rows += 1
@@ -464,11 +526,16 @@ class Picker:
                 m.set_params(row)
                 self.mlp.append(m)
 
-    def ranking(self, coll, P, count, es, dims=None):
-        """Candidate arm indices, best first."""
-        ok = [a for a, arm in enumerate(ARMS) if statically_valid(arm, coll, P, count, dims)]
+    def ranking(self, coll, P, count, es, dims=None, keep=None):
+        """Candidate arm indices, best first.  keep = (variant, ports)
+        restricts them to arms with that variant and port count."""
+        ok = [a for a, arm in enumerate(ARMS) if statically_valid(arm, coll, P, count, dims) and arm_keeps(arm, keep)]
         if self.mlp is None or not ok:
             first = fixed_rule(coll, P, count, es)
+            if keep is not None:
+                seg = ARMS[first][3]
+                same = [a for a in ok if ARMS[a][3] == seg]
+                return same + [a for a in ok if a not in same]
             rest = [a for a in ok if ARMS[a][1] in ("L", "VEC_DOUBLING_BLOCKS") and a != first]
             return [first] + rest
         x = np.zeros((16, IN_DIM), np.float32)
@@ -476,27 +543,59 @@ class Picker:
         t = predict(self.mlp, x)[0, :NARMS]
         return sorted(ok, key=lambda a: t[a])
 
-    def tune(self, comm, coll, count, datatype, trials=3, reps=3):
-        """Times the `trials` best-ranked provable arms once for this call
-        shape on scratch buffers (the caller's data is not touched) and
-        caches the fastest; later choose() calls apply it.  Returns the arm."""
-        import torch
-
+    def _candidates(self, comm, coll, count, datatype, limit):
+        """Provable arms for the call, best first (at most `limit`), and the
+        caller's (variant, ports) when the result bits depend on them."""
         import bine_trees_fugaku_b200 as bine
 
         es = bine.DTYPE_SIZE[datatype]
-        key = (coll, comm.nranks, tuple(comm.dims), count, es)
+        keep = keep_of(comm, coll) if order_bound(coll, datatype, comm.engine, comm.float_order) else None
         cands = []
-        for a in self.ranking(coll, comm.nranks, count, es, comm.dims):
+        for a in self.ranking(coll, comm.nranks, count, es, comm.dims, keep):
             apply_arm(comm, ARMS[a])
             try:
                 comm.plan_verify(coll, count)
             except bine.Unsupported:
                 continue
             cands.append(a)
-            if len(cands) == trials:
+            if len(cands) == limit:
                 break
+        if keep is not None:
+            # The caller's own schedule, restored whatever the outcome; with
+            # no arm of the arm space it must at least run as it is.
+            comm.set_algo(coll, keep[0])
+            comm.set_ports(keep[1])
+            if not cands:
+                comm.plan_verify(coll, count)
+        return cands, keep
+
+    def _apply(self, comm, coll, count, es, a, keep):
+        """Applies arm `a`, or with keep and no arm of the arm space, the
+        fixed rule's segment alone on the caller's schedule."""
+        if a is not None:
+            apply_arm(comm, ARMS[a])
+            return ARMS[a]
+        seg = ARMS[fixed_rule(coll, comm.nranks, count, es)][3]
+        comm.set_segment(seg)
+        return (coll, keep[0], keep[1], seg)
+
+    def tune(self, comm, coll, count, datatype, trials=3, reps=3):
+        """Times the `trials` best-ranked provable arms once for this call
+        shape on scratch buffers (the caller's data is not touched) and
+        caches the fastest; later choose() calls apply it.  Returns the arm.
+        Float sums in the reference's order keep the caller's variant and
+        port count (only the segment is tuned)."""
+        import torch
+
+        import bine_trees_fugaku_b200 as bine
+
+        es = bine.DTYPE_SIZE[datatype]
+        cands, keep = self._candidates(comm, coll, count, datatype, trials)
+        key = (coll, comm.nranks, tuple(comm.dims), count, datatype, keep)
         if not cands:
+            if keep is not None:
+                self.cache[key] = None
+                return self._apply(comm, coll, count, es, None, keep)
             raise bine.Unsupported(bine.ERR_UNSUPPORTED, f"no Bine schedule runs {coll} at P={comm.nranks}")
         se, re = bine.row_counts(coll, count, comm.nranks)
         tdt = {bine.INT32: torch.int32, bine.INT64: torch.int64, bine.FLOAT: torch.float32,
@@ -512,26 +611,22 @@ class Picker:
             if best is None or t < best[0]:
                 best = (t, a)
         self.cache[key] = best[1]
-        apply_arm(comm, ARMS[best[1]])
-        return ARMS[best[1]]
+        return self._apply(comm, coll, count, es, best[1], keep)
 
-    def choose(self, comm, coll, count, es):
-        """Applies the best provable arm to `comm` and returns it."""
+    def choose(self, comm, coll, count, datatype):
+        """Applies the best provable arm to `comm` and returns it.
+        `datatype` is the call's element type (bine.INT32, bine.FLOAT, ...):
+        float sums in the reference's order keep the caller's variant and
+        port count, so the result bits never change."""
         import bine_trees_fugaku_b200 as bine
 
-        key = (coll, comm.nranks, tuple(comm.dims), count, es)
+        es = bine.DTYPE_SIZE[datatype]
+        keep = keep_of(comm, coll) if order_bound(coll, datatype, comm.engine, comm.float_order) else None
+        key = (coll, comm.nranks, tuple(comm.dims), count, datatype, keep)
         if key not in self.cache:
-            self.cache[key] = None
-            for a in self.ranking(coll, comm.nranks, count, es, comm.dims):
-                apply_arm(comm, ARMS[a])
-                try:
-                    comm.plan_verify(coll, count)
-                except bine.Unsupported:
-                    continue
-                self.cache[key] = a
-                break
+            cands, _ = self._candidates(comm, coll, count, datatype, 1)
+            self.cache[key] = cands[0] if cands else None
         a = self.cache[key]
-        if a is None:
+        if a is None and keep is None:
             raise bine.Unsupported(bine.ERR_UNSUPPORTED, f"no Bine schedule runs {coll} at P={comm.nranks}")
-        apply_arm(comm, ARMS[a])
-        return ARMS[a]
+        return self._apply(comm, coll, count, es, a, keep)

@@ -4,7 +4,7 @@ Run in a checkout that has the reference at REF (default: $BINE_REFERENCE,
 else a directory "reference" beside this repository) and the reference
 library built by `make -C oracle ref`:
 
-    python tests/golden/make_golden.py [REF]
+    python tests/golden/make_golden.py [REF] [--large-only]
 
 Fixtures (all outputs of reference code, never hand-written):
   remap_rank.json      simulation/remap_rank.c (compiled from its source)
@@ -14,7 +14,12 @@ Fixtures (all outputs of reference code, never hand-written):
                        for ALLREDUCE on 2x2x2, 4x4x4 and 8x8x8 tori;
   ref_collectives.npz  results and message traces of the reference library
                        (lib/*.cc via oracle/_ref/bine_ref_run) for small
-                       seeded inputs of every MPI-layer variant.
+                       seeded inputs of every MPI-layer variant;
+  ref_large.json       per case of tests/golden/large_cases.py (P = 128,
+                       256, 384, 1024 and the full-size P = 8 allreduce):
+                       whether the reference completed, whether its result
+                       is the MPI result, and SHA-256 digests of its result
+                       rows and message trace.
 """
 import importlib.util
 import json
@@ -32,6 +37,7 @@ sys.path.insert(0, ROOT)
 from oracle import ref  # noqa: E402
 from oracle.common import buffer_counts  # noqa: E402
 from tests.golden.cases import CASES, case_input  # noqa: E402
+from tests.golden import large_cases  # noqa: E402
 
 
 def remap_rank_c(refdir):
@@ -91,12 +97,45 @@ def ref_collectives():
     return arrays
 
 
+def ref_large():
+    """Digests of the reference's results on tests/golden/large_cases.py:
+    per case whether the reference completed, whether its result is the MPI
+    result, and the SHA-256 of the result rows and of the message trace."""
+    out = []
+    for case in large_cases.CASES:
+        x = large_cases.case_input(case)
+        r = ref.run(case["coll"], x, case["count"], variant=case["variant"], dims=case.get("dims"),
+                    ports=case.get("ports", 1), root=case.get("root", 0), family=case.get("family", "BINE"),
+                    distance=case.get("distance"), trace=True, timeout=900, shim_timeout=60)
+        entry = dict(case)
+        entry["ok"] = r.ok
+        if r.ok:
+            t = r.trace
+            entry["digest"] = large_cases.result_digest(case, r.out)
+            entry["trace_digest"] = large_cases.trace_digest(t["src"], t["dst"], t["bytes"].astype(np.int64))
+            entry["messages"] = int(len(t))
+            entry["mpi"] = large_cases.matches_mpi(case, x, r.out)
+        else:
+            entry["status"] = r.info.get("status", [])[:4]
+        print(json.dumps({k: entry[k] for k in ("coll", "variant", "P", "dtype", "count", "ok")}
+                         | {"mpi": entry.get("mpi")}), flush=True)
+        out.append(entry)
+    return out
+
+
 def main():
     repo = os.path.dirname(os.path.dirname(HERE))
-    refdir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
-        "BINE_REFERENCE", os.path.join(os.path.dirname(repo), "reference"))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    refdir = args[0] if args else os.environ.get("BINE_REFERENCE", os.path.join(os.path.dirname(repo), "reference"))
     if not ref.available():
         sys.exit("build the reference first: make -C oracle ref")
+    if "--large-only" not in sys.argv:
+        small(refdir)
+    with open(os.path.join(HERE, "ref_large.json"), "w") as f:
+        json.dump(ref_large(), f, indent=0)
+
+
+def small(refdir):
     with open(os.path.join(HERE, "remap_rank.json"), "w") as f:
         json.dump(remap_rank_c(refdir), f)
     with open(os.path.join(HERE, "binomial_remap.json"), "w") as f:

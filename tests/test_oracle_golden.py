@@ -75,3 +75,64 @@ def test_oracle_matches_live_reference(coll, variant, P):
     a = sorted(zip(msgs["src"].tolist(), msgs["dst"].tolist(), msgs["bytes"].tolist()))
     b = sorted(zip(r.trace["src"].tolist(), r.trace["dst"].tolist(), r.trace["bytes"].tolist()))
     assert a == b
+
+
+def _large_cases():
+    import json
+    import os
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_large.json")
+    with open(path) as f:
+        return json.load(f)
+
+
+LARGE = _large_cases()
+# The restatement runs one thread per rank with per-block messages: cases
+# whose P^2 message counts would take it beyond a few seconds on a CPU are
+# pinned on the GPU only (tests/test_large_parity_gpu.py).
+SLOW = {("allgather", "VEC_DOUBLING_BLOCKS"), ("allreduce", "B"), ("allreduce", "B_COALESCE"),
+        ("reduce", "REDUCE_SCATTER_GATHER"), ("bcast", "SCATTER_ALLGATHER")}
+
+
+def _large_quick(c):
+    return c["P"] <= 256 or ((c["coll"], c["variant"]) not in SLOW and c["P"] <= 1024)
+
+
+@pytest.mark.parametrize("case", [c for c in LARGE if _large_quick(c)],
+                         ids=lambda c: f"{c['coll']}-{c['variant']}-P{c['P']}-{c['dtype']}-n{c['count']}"
+                         + "".join(f"-{k}{c[k]}" for k in ("ports", "root", "family", "dims") if k in c))
+def test_oracle_matches_reference_digests_at_large_p(case):
+    """The restatement against digests of the reference's own results at
+    P = 128..1024 (tests/golden/ref_large.json): identical result bytes and
+    message multiset where the reference gives the MPI result; where it
+    fails or returns other data, the restatement reports the reference as
+    unsupported."""
+    from tests.golden import large_cases as lc
+
+    x = lc.case_input(case)
+    kw = dict(variant=case["variant"], dims=case.get("dims"), ports=case.get("ports", 1), root=case.get("root", 0),
+              family=case.get("family", "BINE"), distance=case.get("distance"))
+    try:
+        out, msgs = port.run(case["coll"], x, case["count"], trace=True, **kw)
+    except port.ReferenceUnsupported:
+        assert not (case["ok"] and case["mpi"]), "the restatement refuses a case the reference runs correctly"
+        return
+    assert case["ok"], "the restatement runs a case the reference fails on"
+    assert lc.result_digest(case, out) == case["digest"]
+    assert lc.trace_digest(msgs["src"], msgs["dst"], msgs["bytes"].astype(np.int64)) == case["trace_digest"]
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference not built (make -C oracle ref)")
+@pytest.mark.parametrize("case", [c for c in LARGE if c["P"] <= 256 and c["ok"] and c["count"] < 1 << 20][::7],
+                         ids=lambda c: f"{c['coll']}-{c['variant']}-P{c['P']}-{c['dtype']}-n{c['count']}")
+def test_large_digests_reproduce_on_the_live_reference(case):
+    """A sample of the large-P fixtures recomputed by the reference library
+    itself (oracle/_ref): the digests are current."""
+    from tests.golden import large_cases as lc
+
+    x = lc.case_input(case)
+    r = ref.run(case["coll"], x, case["count"], variant=case["variant"], dims=case.get("dims"),
+                ports=case.get("ports", 1), root=case.get("root", 0), family=case.get("family", "BINE"),
+                distance=case.get("distance"), timeout=300, shim_timeout=60)
+    assert r.ok, r.stderr[-500:]
+    assert lc.result_digest(case, r.out) == case["digest"]

@@ -77,12 +77,12 @@ def test_picker_without_weights_falls_back_past_refused_arms():
     planner refuses it, and the picker falls back to the L tree."""
     p = pk.Picker(path=None)
     comm = bine.Comm(23)
-    arm = p.choose(comm, "allreduce", 95239, 4)
+    arm = p.choose(comm, "allreduce", 95239, bine.INT32)
     assert arm[1] == "L"
     comm.plan_verify("allreduce", 95239)
     comm.close()
     comm = bine.Comm(64)
-    assert p.choose(comm, "allreduce", 1 << 20, 4) == ("allreduce", "B", 6, 65536)
+    assert p.choose(comm, "allreduce", 1 << 20, bine.INT32) == ("allreduce", "B", 6, 65536)
     comm.close()
 
 
@@ -92,7 +92,7 @@ def test_picker_reports_when_nothing_runs():
     p = pk.Picker(path=None)
     comm = bine.Comm(91)
     with pytest.raises(bine.Unsupported):
-        p.choose(comm, "reduce_scatter", 852, 4)
+        p.choose(comm, "reduce_scatter", 852, bine.INT32)
     comm.close()
 
 
@@ -146,3 +146,39 @@ def test_saved_weights_are_the_bf16_forward_values(tmp_path):
     assert p.shape == (2, 5) and meta["models"] == 2
     assert dims == (pk.IN_DIM, 256, pk.OUT_DIM) and [tuple(a) for a in arms] == pk.ARMS
     assert json.dumps(st) and meta["calls"] == 0
+
+
+def test_picker_keeps_variant_and_ports_of_reference_order_float_sums():
+    """A float32 sum in the reference's order is a different addition tree
+    per variant and port count, so the picker chooses only the segment for
+    it; integer calls and FAST-order calls on the FUSED engine are free."""
+    p = pk.Picker(path=None)
+    comm = bine.Comm(64)
+    comm.set_engine("steps")
+    comm.set_algo("allreduce", "L")
+    comm.set_ports(2)
+    arm = p.choose(comm, "allreduce", 1 << 20, bine.FLOAT)
+    assert arm[:3] == ("allreduce", "L", 2)
+    assert (comm.algo["allreduce"], comm.ports) == ("L", 2)
+    free = bine.Comm(64)
+    free.set_engine("steps")
+    assert p.choose(free, "allreduce", 1 << 20, bine.INT32) == ("allreduce", "B", 6, 65536)
+    fast = bine.Comm(64)
+    fast.set_float_order("fast")
+    assert p.choose(fast, "allreduce", 1 << 20, bine.FLOAT) == ("allreduce", "B", 6, 65536)
+    assert pk.order_bound("allreduce", bine.FLOAT, "fused", "reference")
+    assert pk.order_bound("reduce_scatter", bine.DOUBLE, "pipelined", "fast")
+    assert not pk.order_bound("allreduce", bine.FLOAT, "fused", "fast")
+    assert not pk.order_bound("allgather", bine.FLOAT, "steps", "reference")
+    assert not pk.order_bound("allreduce", bine.INT64, "steps", "reference")
+    for c in (comm, free, fast):
+        c.close()
+
+
+def test_evaluation_restricts_float_reductions_to_the_segment_choice():
+    cfg = {"coll": "allreduce", "P": 64, "count": 1 << 20, "es": 4, "dtype": "float"}
+    m = pk.allowed_arms(cfg)
+    fa = pk.ARMS[pk.fixed_rule("allreduce", 64, 1 << 20, 4)]
+    assert m.sum() == len(pk.SEGMENTS)
+    assert all(pk.ARMS[a][1:3] == fa[1:3] for a in np.nonzero(m)[0])
+    assert pk.allowed_arms(dict(cfg, dtype="int32")).all()

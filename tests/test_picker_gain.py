@@ -100,7 +100,7 @@ def test_shortlist_tuning_keeps_the_fastest_of_three_and_the_call_is_correct():
     comm = bine.Comm(128)
     comm.set_engine("steps")
     arm = picker.tune(comm, "allreduce", 1 << 15, bine.INT32, trials=3)
-    assert picker.choose(comm, "allreduce", 1 << 15, 4) == arm
+    assert picker.choose(comm, "allreduce", 1 << 15, bine.INT32) == arm
     x = torch.randint(-1000, 1001, (128, 1 << 15), dtype=torch.int32, device="cuda")
     y = torch.zeros_like(x)
     comm.allreduce(x, y, 1 << 15, bine.INT32)
@@ -117,11 +117,43 @@ def test_runtime_picker_applies_a_provable_arm_and_the_call_is_correct():
     for P, count in ((64, 1 << 16), (23, 4096), (256, 1 << 12)):
         comm = bine.Comm(P)
         comm.set_engine("steps")
-        arm = picker.choose(comm, "allreduce", count, 4)
+        arm = picker.choose(comm, "allreduce", count, bine.INT32)
         assert arm[0] == "allreduce"
         x = torch.randint(-1000, 1001, (P, count), dtype=torch.int32, device="cuda")
         y = torch.zeros_like(x)
         comm.allreduce(x, y, count, bine.INT32)
         comm.synchronize()
         assert torch.equal(y, x.sum(0, dtype=torch.int32).expand(P, count))
+        comm.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine", ["steps", "fused"])
+def test_picker_never_changes_float32_result_bits(engine):
+    """A float32 allreduce in the reference's order gives the same bits with
+    and without Picker.choose / Picker.tune: the picker keeps the caller's
+    variant and port count and chooses only the segment."""
+    import torch
+
+    picker = pk.Picker()
+    for P, count, variant, ports in ((64, 1 << 16, "B", 1), (23, 4096, "L", 1), (256, 1 << 12, "B", 1),
+                                     (16, 5000, "L", 2), (128, 1 << 14, "B_COALESCE", 6)):
+        comm = bine.Comm(P)
+        comm.set_engine(engine)
+        comm.set_algo("allreduce", variant)
+        comm.set_ports(ports)
+        x = torch.randn((P, count), dtype=torch.float32, device="cuda")
+        want = torch.zeros_like(x)
+        comm.allreduce(x, want, count, bine.FLOAT)
+        comm.synchronize()
+        arm = picker.choose(comm, "allreduce", count, bine.FLOAT)
+        assert arm[1:3] == (variant, ports)
+        for step in range(2):
+            if step:
+                arm = picker.tune(comm, "allreduce", count, bine.FLOAT, trials=2)
+                assert arm[1:3] == (variant, ports)
+            got = torch.zeros_like(x)
+            comm.allreduce(x, got, count, bine.FLOAT)
+            comm.synchronize()
+            assert torch.equal(got.view(torch.int32), want.view(torch.int32)), (P, variant, ports, arm)
         comm.close()
