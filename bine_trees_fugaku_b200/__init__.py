@@ -25,7 +25,7 @@ SUCCESS, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_INTERNA
 WINDOW_HOOK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong)
 ENGINE_FUSED, ENGINE_STEPS, ENGINE_PIPELINED = 0, 1, 2
 ORDER_REFERENCE, ORDER_FAST = 0, 1
-FAMILY = {"BINE": 1, "RECDOUB": 2, "BRUCK": 3}
+FAMILY = {"BINE": 1, "RECDOUB": 2, "BRUCK": 3, "RING": 4}
 DISTANCE = {None: -1, "INCREASING": 0, "DECREASING": 1}
 
 COLLS = ["allreduce", "reduce_scatter", "allgather", "bcast", "reduce", "alltoall", "scatter", "gather"]

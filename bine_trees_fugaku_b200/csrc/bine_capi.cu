@@ -1784,7 +1784,8 @@ int bine_comm_set_ports(bine_comm_t comm, int ports) {
 int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int family, int distance) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     if ((int)coll < 0 || (int)coll >= kNumColls) return fail(BINE_ERR_ARG, "invalid collective");
-    if (family != BINE_FAMILY_BINE && family != BINE_FAMILY_RECDOUB && family != BINE_FAMILY_BRUCK)
+    if (family != BINE_FAMILY_BINE && family != BINE_FAMILY_RECDOUB && family != BINE_FAMILY_BRUCK &&
+        family != BINE_FAMILY_RING)
         return fail(BINE_ERR_ARG, "invalid family");
     if (family == BINE_FAMILY_BRUCK && coll != BINE_COLL_ALLTOALL)
         return fail(BINE_ERR_ARG, "the BRUCK family is an alltoall algorithm");
@@ -2078,7 +2079,7 @@ int bine_link_bytes(bine_comm_t comm, bine_coll_t coll, long count, bine_datatyp
     bool mirrored = false;
     for (int p = 0; p < comm->ports; p++) mirrored |= mirrored_port(p, t.ndims);
     int kind = -1;
-    if (all_p2 && (cf.family == kFamilyBine || !mirrored)) {
+    if (all_p2 && cf.family != kFamilyRing && (cf.family == kFamilyBine || !mirrored)) {
         if (coll == kAllreduce && (cf.variant == kArB || cf.variant == kArBCoalesce) && cf.distance == kIncreasing &&
             count >= (long)comm->ports * t.size)
             kind = 0;

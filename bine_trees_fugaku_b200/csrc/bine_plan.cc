@@ -1112,6 +1112,131 @@ void gen_alltoall_bruck(const Gen& g) {
     b.finish(g.s);
 }
 
+// Bucket allreduce, the reference's RING family: the multi-dimensional ring
+// the paper compares Bine against (BineCommon::bucket_allreduce,
+// lib/libbine_common.cc:2486-2663, over ringRedScatAG,
+// lib/libbine_common.cc:2372-2484).  The reference runs it on uTofu only;
+// this restates its schedule as messages.
+//   * The vector, padded to a multiple of 2*D*P elements, is copied into a
+//     work row (lib/libbine_common.cc:2559) and cut into 2*D buckets; bucket
+//     2i runs its rings toward the next node of a dimension, bucket 2i+1
+//     toward the previous one (lib/libbine_common.cc:2598-2603).
+//   * Reduce-scatter rounds s = 0..D-1: bucket pair i reduces its current
+//     range along dimension (i + s) % D with a ring reduce-scatter (n - 1
+//     steps; at step k a rank sends chunk c - k - 1 and adds the received
+//     chunk c - k - 2 into its own, or c + k + 1 and c + k + 2 toward the
+//     previous node; lib/libbine_common.cc:2395-2402), then keeps chunk c
+//     (its coordinate) as the next round's range (lib/libbine_common.cc:
+//     2617-2620).
+//   * Allgather rounds in reverse order: the first copies each bucket's
+//     range from the work row to the receive row (lib/libbine_common.cc:
+//     2648-2656), then ring allgathers (chunk c - k sent, c - k - 1
+//     received, or c + k and c + k + 1; lib/libbine_common.cc:2435-2441)
+//     rebuild the ranges in the receive row.
+// Moves and messages cover the real elements only: the padding past `count`
+// (uninitialised in the reference) feeds no result, and the reference's
+// allgather skips it too (lib/libbine_common.cc:2452-2466).
+void gen_allreduce_ring(const Gen& g) {
+    const Torus& t = g.t;
+    const int P = g.P, D = t.ndims;
+    const int64_t count = g.k.count;
+    int64_t padded = count;
+    const int64_t unit = 2LL * D * P;
+    if (padded % unit) padded += unit - padded % unit;
+    const int64_t B = padded / (2 * D);
+    g.s->send_elems = g.s->recv_elems = count;
+    Builder b(P, padded);
+    auto clip = [&](int64_t off, int64_t n) { return std::max<int64_t>(0, std::min(n, count - off)); };
+    b.begin();
+    for (int r = 0; r < P; r++) b.copy(R(r, kBufTmp, 0), R(r, kBufSend, 0), count);
+    b.end(g.s);
+    std::vector<std::vector<int>> coord(P, std::vector<int>(kMaxDims, 0));
+    for (int r = 0; r < P; r++) t.coords(r, coord[r].data());
+    auto neighbour = [&](int r, int d, int delta) {
+        int c[kMaxDims];
+        for (int i = 0; i < kMaxDims; i++) c[i] = coord[r][i];
+        c[d] = pmod(c[d] + delta, t.dims[d]);
+        return t.id(c);
+    };
+    // Per bucket pair i and rank r: the current range's offset inside the
+    // bucket; per round and pair: the range size and dimension.
+    std::vector<std::vector<int64_t>> offset(D, std::vector<int64_t>(P, 0));
+    std::vector<int64_t> size(D, B);
+    std::vector<std::vector<std::vector<int64_t>>> saved_off(D);  // [round][pair][rank]
+    std::vector<std::vector<int64_t>> saved_size(D, std::vector<int64_t>(D));
+    const int tag0 = 0x7000;
+    for (int s = 0; s < D; s++) {
+        saved_off[s] = offset;
+        int most = 0;
+        for (int i = 0; i < D; i++) {
+            saved_size[s][i] = size[i];
+            most = std::max(most, t.dims[(i + s) % D]);
+        }
+        for (int k = 0; k + 1 < most; k++) {
+            b.begin();
+            for (int j = 0; j < 2 * D; j++) {
+                const int i = j / 2, d = (i + s) % D, n = t.dims[d];
+                if (k + 1 >= n) continue;
+                const int64_t seg = size[i] / n;
+                for (int r = 0; r < P; r++) {
+                    const int c = coord[r][d];
+                    const int to = neighbour(r, d, j % 2 ? -1 : 1), from = neighbour(r, d, j % 2 ? 1 : -1);
+                    const int send_chunk = j % 2 ? pmod(c + 1 + k, n) : pmod(c - k - 1, n);
+                    const int recv_chunk = j % 2 ? pmod(c + 2 + k, n) : pmod(c - k - 2, n);
+                    const int64_t base = j * B + offset[i][r];
+                    const int64_t so = base + send_chunk * seg, ro = base + recv_chunk * seg;
+                    if (clip(so, seg) > 0) b.send(r, to, tag0 + j, R(r, kBufTmp, so), clip(so, seg));
+                    if (clip(ro, seg) > 0) {
+                        Region into = R(r, kBufTmp, ro);
+                        b.recv(r, from, tag0 + j, into, clip(ro, seg), &into);
+                    }
+                }
+            }
+            b.end(g.s);
+        }
+        if (s != D - 1)
+            for (int i = 0; i < D; i++) {
+                const int d = (i + s) % D;
+                size[i] /= t.dims[d];
+                for (int r = 0; r < P; r++) offset[i][r] += coord[r][d] * size[i];
+            }
+    }
+    for (int s = D - 1; s >= 0; s--) {
+        if (s == D - 1) {
+            b.begin();
+            for (int j = 0; j < 2 * D; j++)
+                for (int r = 0; r < P; r++) {
+                    const int64_t o = j * B + saved_off[s][j / 2][r];
+                    if (clip(o, saved_size[s][j / 2]) > 0)
+                        b.copy(R(r, kBufRecv, o), R(r, kBufTmp, o), clip(o, saved_size[s][j / 2]));
+                }
+            b.end(g.s);
+        }
+        int most = 0;
+        for (int i = 0; i < D; i++) most = std::max(most, t.dims[(i + s) % D]);
+        for (int k = 0; k + 1 < most; k++) {
+            b.begin();
+            for (int j = 0; j < 2 * D; j++) {
+                const int i = j / 2, d = (i + s) % D, n = t.dims[d];
+                if (k + 1 >= n) continue;
+                const int64_t seg = saved_size[s][i] / n;
+                for (int r = 0; r < P; r++) {
+                    const int c = coord[r][d];
+                    const int to = neighbour(r, d, j % 2 ? -1 : 1), from = neighbour(r, d, j % 2 ? 1 : -1);
+                    const int send_chunk = j % 2 ? pmod(c + k, n) : pmod(c - k, n);
+                    const int recv_chunk = j % 2 ? pmod(c + k + 1, n) : pmod(c - k - 1, n);
+                    const int64_t base = j * B + saved_off[s][i][r];
+                    const int64_t so = base + send_chunk * seg, ro = base + recv_chunk * seg;
+                    if (clip(so, seg) > 0) b.send(r, to, tag0 + 2 * D + j, R(r, kBufRecv, so), clip(so, seg));
+                    if (clip(ro, seg) > 0) b.recv(r, from, tag0 + 2 * D + j, R(r, kBufRecv, ro), clip(ro, seg));
+                }
+            }
+            b.end(g.s);
+        }
+    }
+    b.finish(g.s);
+}
+
 // Scatter down a negabinary binomial tree with wrap-around block ranges
 // (bine_scatter_mpi, lib/libbine_coll_scatter.cc:187-324).  Interior ranks
 // keep the blocks of their subtree in the workspace.
@@ -1478,9 +1603,19 @@ bool Planner::build(const PlanKey& k, Schedule* out, std::string* err) const {
         if (k.root < 0 || k.root >= t_.size) throw PlanError("root out of range");
         if (k.family == kFamilyBruck && k.coll != kAlltoall)
             throw PlanError("the BRUCK family exists for alltoall only; the other entry points assert on it (e.g. lib/libbine.cc:1059, 1146, 1247)");
+        if (k.family == kFamilyRing && k.coll != kAllreduce)
+            throw PlanError(k.coll == kReduceScatter
+                                ? "the RING reduce_scatter (bucket_reduce_scatter) never writes the caller's receive "
+                                  "buffer: it points recvbuf at its own work area (lib/libbine_coll_reduce_scatter.cc:826, 832)"
+                                : (k.coll == kAllgather
+                                       ? "the RING allgather (bucket_allgather) gathers from a work area it never "
+                                         "fills from sendbuf (lib/libbine_coll_allgather.cc:1514-1524)"
+                                       : "the RING family exists for allreduce, reduce_scatter and allgather only; "
+                                         "the other entry points assert on it (e.g. lib/libbine.cc:1284-1285)"));
         switch (k.coll) {
         case kAllreduce:
-            if (k.variant == kArL) gen_allreduce_l(g);
+            if (k.family == kFamilyRing) gen_allreduce_ring(g);
+            else if (k.variant == kArL) gen_allreduce_l(g);
             else if (k.variant == kArB || k.variant == kArBCoalesce || k.variant == kArBCont) gen_allreduce_b(g);
             else throw PlanError("unknown allreduce variant");
             break;

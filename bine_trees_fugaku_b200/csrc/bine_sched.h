@@ -187,7 +187,7 @@ BINE_HD bool mirrored_port(int port, int ndims) {
     return false;
 }
 
-enum Family { kFamilyBine = 1, kFamilyRecDoub = 2, kFamilyBruck = 3 };  // lib/libbine_common.h:77-85
+enum Family { kFamilyBine = 1, kFamilyRecDoub = 2, kFamilyBruck = 3, kFamilyRing = 4 };  // lib/libbine_common.h:77-85
 
 // Dimension and in-dimension step of each global step for a port: dimensions
 // are visited round-robin starting at port % ndims, skipping exhausted ones.

@@ -78,10 +78,14 @@ enum {
     BINE_ALLTOALL_LOG = 0, BINE_SCATTER_BINOMIAL_TREE = 0, BINE_GATHER_BINOMIAL_TREE = 0
 };
 
-/* LIBBINE_<COLL>_ALGO_FAMILY and LIBBINE_<COLL>_DISTANCE. */
 /* LIBBINE_<COLL>_ALGO_FAMILY (lib/libbine_common.h:77-85).  BRUCK is the
- * reference's comparator for alltoall (lib/libbine_coll_alltoall.cc:18). */
-enum { BINE_FAMILY_BINE = 1, BINE_FAMILY_RECDOUB = 2, BINE_FAMILY_BRUCK = 3 };
+ * reference's comparator for alltoall (lib/libbine_coll_alltoall.cc:18);
+ * RING is its comparator for allreduce, the multi-dimensional bucket ring
+ * (lib/libbine_common.cc:2372-2663; the variant is ignored, as in the
+ * reference's dispatch, lib/libbine.cc:1056-1057).  RING reduce_scatter and
+ * allgather return BINE_ERR_UNSUPPORTED: the reference's versions never
+ * deliver the result. */
+enum { BINE_FAMILY_BINE = 1, BINE_FAMILY_RECDOUB = 2, BINE_FAMILY_BRUCK = 3, BINE_FAMILY_RING = 4 };
 enum { BINE_DISTANCE_INCREASING = 0, BINE_DISTANCE_DECREASING = 1, BINE_DISTANCE_DEFAULT = -1 };
 
 /* Execution engines.

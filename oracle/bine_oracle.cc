@@ -1272,6 +1272,111 @@ void alltoall_bruck(const Ctx& c, int r) {
     for (int i = 0; i < size; i++) std::memcpy(recvbuf + (size_t)mod(r - i, size) * cb, tsend.data() + i * cb, cb);
 }
 
+// --------------------------------------------------- bucket (ring) allreduce
+// BineCommon::bucket_allreduce (lib/libbine_common.cc:2486-2663) with
+// ringRedScatAG (lib/libbine_common.cc:2372-2484), the RING family's
+// allreduce, restated over this file's message layer in place of uTofu puts.
+// The reference ships whole segments, padding past the real count included
+// (its padding is uninitialised and feeds no result); here every message and
+// reduction covers the real elements only.
+void ring_red_scat_ag(const Ctx& c, int r, char* data, long real, long off, long cnt, int nproc, int rank,
+                      int recvfrom, int sendto, int redscat, int tag) {
+    const long seg = cnt / nproc;  // cnt is a multiple of nproc (lib/libbine_common.cc:2376-2387)
+    auto clip = [&](long o) { return std::max(0L, std::min(seg, real - o)); };
+    std::vector<char> buffer((size_t)seg * c.es + 1);
+    for (int i = 0; i < nproc - 1; i++) {
+        int recv_chunk, send_chunk;
+        if (redscat == 0) {
+            recv_chunk = mod(rank - i - 2, nproc);
+            send_chunk = mod(rank - i - 1, nproc);
+        } else if (redscat == 1) {
+            recv_chunk = (rank + 2 + i) % nproc;
+            send_chunk = (rank + 1 + i) % nproc;
+        } else if (redscat == 2) {
+            recv_chunk = mod(rank - i - 1, nproc);
+            send_chunk = mod(rank - i, nproc);
+        } else {
+            recv_chunk = (rank + i + 1) % nproc;
+            send_chunk = (rank + i) % nproc;
+        }
+        const long so = off + send_chunk * seg, ro = off + recv_chunk * seg;
+        if (clip(so) > 0) c.world->send(r, sendto, tag, data + so * c.es, (size_t)clip(so) * c.es);
+        if (clip(ro) > 0) {
+            if (redscat < 2) {
+                c.world->recv(r, recvfrom, tag, buffer.data(), (size_t)clip(ro) * c.es);
+                mpi_reduce_local(c.call->dtype, buffer.data(), data + ro * c.es, (size_t)clip(ro));
+            } else {
+                c.world->recv(r, recvfrom, tag, data + ro * c.es, (size_t)clip(ro) * c.es);
+            }
+        }
+    }
+}
+
+void bucket_allreduce(const Ctx& c, int r) {
+    const int D = c.topo.D, size = c.P;
+    const long real = c.count;
+    long count = real;
+    while (count % ((2L * D) * size)) count += 1;
+    std::vector<char> data((size_t)count * c.es + 1, 0);
+    char* recvbuf = out_of(c, r);
+    std::memcpy(data.data(), in_of(c, r), (size_t)real * c.es);
+    int relcoord[3] = {0, 0, 0}, sendto[3], recvfrom[3];
+    c.topo.coord(r, relcoord);
+    for (int i = 0; i < D; i++) {
+        int coord[3] = {relcoord[0], relcoord[1], relcoord[2]};
+        coord[i] = (relcoord[i] + 1) % c.topo.dims[i];
+        sendto[i] = c.topo.id(coord);
+        coord[i] = (relcoord[i] - 1 + c.topo.dims[i]) % c.topo.dims[i];
+        recvfrom[i] = c.topo.id(coord);
+    }
+    std::vector<long> data_size(D, count / (2 * D)), offsets(D, 0);
+    std::vector<long> loop_off_l(D * D), loop_off_r(D * D), loop_size(D * D);
+    for (int s = 0; s < D; s++) {
+        // Every bucket's ring of this round (the reference runs them on
+        // concurrent threads over disjoint ranges).
+        std::vector<std::function<void()>> rings;
+        for (int i = 0; i < D; i++) {
+            const int d = (i + s) % D;
+            const long ol = (2L * i) * (count / (2 * D)) + offsets[i], orr = (2L * i + 1) * (count / (2 * D)) + offsets[i];
+            loop_off_l[s * D + i] = ol;
+            loop_off_r[s * D + i] = orr;
+            loop_size[s * D + i] = data_size[i];
+            const long sz = data_size[i];
+            const int n = c.topo.dims[d], rc = relcoord[d];
+            rings.push_back([&, ol, sz, n, rc, d, i]() {
+                ring_red_scat_ag(c, r, data.data(), real, ol, sz, n, rc, recvfrom[d], sendto[d], 0, 0x7000 + 2 * i);
+            });
+            rings.push_back([&, orr, sz, n, rc, d, i]() {
+                ring_red_scat_ag(c, r, data.data(), real, orr, sz, n, rc, sendto[d], recvfrom[d], 1, 0x7000 + 2 * i + 1);
+            });
+            if (s != D - 1) {
+                data_size[i] /= n;
+                offsets[i] += relcoord[d] * data_size[i];
+            }
+        }
+        for (auto& f : rings) f();
+    }
+    for (int s = D - 1; s >= 0; s--) {
+        if (s == D - 1)
+            for (int j = 0; j < 2 * D; j++) {
+                const long o = j % 2 ? loop_off_r[s * D + j / 2] : loop_off_l[s * D + j / 2];
+                if (o < real) {
+                    long ct = loop_size[s * D + j / 2];
+                    if (o + ct > real) ct = real - o;
+                    std::memcpy(recvbuf + o * c.es, data.data() + o * c.es, (size_t)ct * c.es);
+                }
+            }
+        for (int i = D - 1; i >= 0; i--) {
+            const int d = (i + s) % D, n = c.topo.dims[d], rc = relcoord[d];
+            const long sz = loop_size[s * D + i];
+            ring_red_scat_ag(c, r, recvbuf, real, loop_off_l[s * D + i], sz, n, rc, recvfrom[d], sendto[d], 2,
+                             0x7000 + 2 * D + 2 * i);
+            ring_red_scat_ag(c, r, recvbuf, real, loop_off_r[s * D + i], sz, n, rc, sendto[d], recvfrom[d], 3,
+                             0x7000 + 2 * D + 2 * i + 1);
+        }
+    }
+}
+
 // ----------------------------------------------------------- scatter/gather
 // bine_scatter_mpi (lib/libbine_coll_scatter.cc:187-324).
 void scatter_tree(const Ctx& c, int r) {
@@ -1504,7 +1609,9 @@ int oracle_run(const oracle_call_t* call, const void* in, void* out, oracle_msg_
         bool all_p2 = true;
         switch (call->coll) {
         case OR_ALLREDUCE: {
-            if (call->algo == OR_AR_L) {
+            if (call->family == OR_FAMILY_RING) {
+                body = [&](int r) { bucket_allreduce(c, r); };
+            } else if (call->algo == OR_AR_L) {
                 int vd[3];
                 for (int i = 0; i < c.topo.D; i++) {
                     int st = ceil_log2(c.topo.dims[i]);

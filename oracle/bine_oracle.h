@@ -46,7 +46,7 @@ enum {
 };
 
 /* Algorithm families (lib/libbine_common.h:75-86). */
-enum { OR_FAMILY_BINE = 1, OR_FAMILY_RECDOUB = 2, OR_FAMILY_BRUCK = 3 };
+enum { OR_FAMILY_BINE = 1, OR_FAMILY_RECDOUB = 2, OR_FAMILY_BRUCK = 3, OR_FAMILY_RING = 4 };
 
 /* Distance types (lib/libbine_common.h:65-68). */
 enum { OR_DIST_INCREASING = 0, OR_DIST_DECREASING = 1 };

@@ -26,7 +26,7 @@ DEFAULT_VARIANT = {"allreduce": "B", "allgather": "VEC_DOUBLING_CONT_PERMUTE",
                    "reduce_scatter": "VEC_HALVING_CONT_PERMUTE", "bcast": "BINOMIAL_TREE",
                    "reduce": "BINOMIAL_TREE", "alltoall": "LOG", "scatter": "BINOMIAL_TREE_CONT_PERMUTE",
                    "gather": "BINOMIAL_TREE_CONT_PERMUTE"}
-FAMILIES = {"BINE": 1, "RECDOUB": 2, "BRUCK": 3}
+FAMILIES = {"BINE": 1, "RECDOUB": 2, "BRUCK": 3, "RING": 4}
 
 
 def buffer_counts(coll, count, P):

@@ -282,6 +282,7 @@ def test_step_engine_barrier_timeout_is_reported_and_recoverable(engine):
     ([4, 4, 4], "allreduce", "L", 1, "RECDOUB"), ([8, 8], "allreduce", "B", 1, "RECDOUB"),
     ([4, 8], "allgather", "VEC_DOUBLING_CONT_PERMUTE", 1, "BINE"), ([6, 4], "allreduce", "B", 1, "BINE"),
     ([4, 4, 4], "alltoall", "LOG", 1, "BINE"), ([16], "bcast", "BINOMIAL_TREE", 1, "BINE"),
+    ([4, 4], "allreduce", "B", 1, "RING"), ([2, 4, 8], "allreduce", "B", 1, "RING"),
 ])
 def test_device_link_bytes_match_host(dims, coll, variant, ports, family):
     P = int(np.prod(dims))
@@ -581,3 +582,20 @@ def test_overlapping_arrays_match_separate_arrays(engine, coll, layout):
             comm.synchronize()
             got = recv.view(P, rc).cpu().numpy()
             assert np.array_equal(got[rr].view(np.uint32), want[rr].view(np.uint32)), (dt, layout)
+
+
+@pytest.mark.parametrize("engine", ["fused", "steps", "pipelined"])
+@pytest.mark.parametrize("dims,count", [([8], 1000), ([4, 4], 77), ([2, 3, 4], 1001), ([256], 256 * 2 * 64 + 3),
+                                        ([8, 8, 4], 256 * 6 * 8 + 1), ([6], 5)])
+def test_ring_allreduce_matches_the_oracle(engine, dims, count):
+    """The bucket (ring) allreduce, the reference's RING family, on every
+    engine: the oracle's bytes, float32 in its addition order included."""
+    P = int(np.prod(dims))
+    comm = make_comm(P, "allreduce", "B", dims=dims if len(dims) > 1 else None, family="RING", engine=engine)
+    for dt in (np.int32, np.float32):
+        rng = np.random.default_rng(P + count)
+        x = (rng.integers(-1000, 1001, (P, count)) if dt == np.int32 else rng.standard_normal((P, count))).astype(dt)
+        want, _ = port.run("allreduce", x, count, family="RING", dims=dims if len(dims) > 1 else None)
+        got = run(comm, "allreduce", x, count)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), dt
+    comm.close()
