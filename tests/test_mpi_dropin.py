@@ -60,7 +60,7 @@ def test_without_a_gpu_every_rank_reports_the_error():
         pytest.skip("a GPU is present")
     binary = build()
     x = np.arange(4 * 64, dtype=np.int32).reshape(4, 64)
-    r = ref.run("allreduce", x, 64, binary=binary, timeout=60, shim_timeout=10)
+    r = ref.run("allreduce", x, 64, binary=binary, timeout=180, shim_timeout=60)
     assert not r.ok
     assert r.info["status"] == ["exit:1"] * 4
     assert "bine_mpi:" in r.stderr
