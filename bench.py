@@ -1170,16 +1170,29 @@ def run_picker_suite(args):
     # Pick latency: one forward pass of a 16-row batch through every model
     # of the ensemble, device-timed.
     x16 = torch.from_numpy(X[:16].copy() if len(X) >= 16 else np.zeros((16, pk.IN_DIM), np.float32)).cuda()
+    ens = bine.Ensemble(mlps)
+    y16 = torch.empty((16, pk.OUT_DIM), dtype=torch.float32, device="cuda")
     for _ in range(5):
-        for m in mlps:
-            m.forward(x16)
+        ens.forward(x16, out=y16)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(100):
-        for m in mlps:
-            m.forward(x16)
+        ens.forward(x16, out=y16)
     e1.record()
     torch.cuda.synchronize()
+    # The layered path (per model: one GEMM + bias/GELU launch per layer),
+    # for comparison.
+    for _ in range(3):
+        for m in mlps:
+            m.forward(x16)
+    l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0.record()
+    for _ in range(100):
+        for m in mlps:
+            m.forward(x16)
+    l1.record()
+    torch.cuda.synchronize()
+    ens.close()
     meta = {"calls": len(cfgs), "held_out": int(len(te)), "train_steps": args.picker_steps,
             "single_model_pick_within_5pct": single["pick_within_5pct_of_optimum"],
             "device": torch.cuda.get_device_name(0)}
@@ -1189,7 +1202,11 @@ def run_picker_suite(args):
             "noise_ceiling": ceiling, "calls_measured": len(cfgs), "arms": pk.NARMS,
             "valid_arms_per_call_mean": float(valid.sum(1).mean()) if len(cfgs) else 0.0,
             "train_loss_first_last": [losses[0], float(np.mean(losses[-50:]))],
-            "measure_s": t_measure, "train_s": t_train, "forward16_us": e0.elapsed_time(e1) * 10.0,
+            "measure_s": t_measure, "train_s": t_train,
+            "forward16_us": e0.elapsed_time(e1) * 10.0,
+            "forward16_layered_us": l0.elapsed_time(l1) * 10.0,
+            "forward16_note": "ensemble mean of a 16-row batch: one fused launch (bine_mlp_ensemble_forward) "
+                              "against the layered per-model path",
             "config": {"model": "ensemble of bine_mlp 16-256-256-256-%d GELU, bf16 weights, fp32 accumulate" % pk.OUT_DIM,
                        "engine": "steps", "timing": "per arm: median of 3 CUDA-event batches of back-to-back "
                                                     "launches (each batch ~300 us, at most 32 launches)",

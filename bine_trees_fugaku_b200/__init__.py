@@ -143,6 +143,9 @@ def lib():
         "bine_mlp_forward": [vp, vp, i, vp, vp],
         "bine_mlp_gradients": [vp, vp, vp, vp, i, vp, ctypes.POINTER(ctypes.c_float)],
         "bine_mlp_train_step": [vp, vp, vp, vp, i, ctypes.c_float, vp, ctypes.POINTER(ctypes.c_float)],
+        "bine_mlp_ensemble_create": [ctypes.POINTER(vp), i, ctypes.POINTER(vp)],
+        "bine_mlp_ensemble_forward": [vp, vp, i, vp, vp],
+        "bine_mlp_ensemble_destroy": [vp],
         "bine_batch_create": [ctypes.POINTER(BatchItem), i, ctypes.POINTER(BatchTuning), ctypes.POINTER(vp)],
         "bine_batch_launch": [vp, vp],
         "bine_batch_destroy": [vp],
@@ -560,6 +563,41 @@ class MLP:
     def close(self):
         if getattr(self, "_h", None):
             lib().bine_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Ensemble:
+    """bine_mlp_ensemble_*: the mean output of 1..8 MLPs of one shape
+    (hidden width 256), computed by one fused launch."""
+
+    def __init__(self, mlps):
+        self.mlps = list(mlps)
+        self.dims = self.mlps[0].dims
+        arr = (ctypes.c_void_p * len(self.mlps))(*[m._h.value for m in self.mlps])
+        self._h = ctypes.c_void_p()
+        self._check(lib().bine_mlp_ensemble_create(arr, len(self.mlps), ctypes.byref(self._h)))
+
+    def _check(self, rc):
+        if rc != SUCCESS:
+            raise BineError(rc, lib().bine_mlp_last_error().decode())
+
+    def forward(self, x, stream=None, out=None):
+        """x: CUDA float32 tensor [n, in] (n multiple of 16) -> mean [n, out]."""
+        import torch
+        y = out if out is not None else torch.empty((x.shape[0], self.dims[2]), dtype=torch.float32, device=x.device)
+        h = stream.cuda_stream if stream is not None else 0
+        self._check(lib().bine_mlp_ensemble_forward(self._h, x.data_ptr(), x.shape[0], y.data_ptr(), h))
+        return y
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bine_mlp_ensemble_destroy(self._h)
             self._h = None
 
     def __del__(self):

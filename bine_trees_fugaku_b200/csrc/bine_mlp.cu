@@ -13,6 +13,7 @@
 //   backward: d_pre = d_act * gelu'(pre) (rounded to bf16 for the GEMMs),
 //             dW_l = d_pre^T act_{l-1}, db_l = column sums, d_act_{l-1} = d_pre W_l
 //   update:   Adam on fp32 master weights, refreshed bf16 copies.
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <mma.h>
@@ -165,6 +166,131 @@ __global__ void k_adam(float* w, const float* g, float* m, float* v, bf16* wb, l
 }
 
 unsigned grid1(long long n) { return (unsigned)std::max(1LL, std::min((n + 255) / 256, 148LL * 8)); }
+
+// ------------------------------------------------- fused ensemble inference
+// The picker evaluates a handful of models on one 16-row batch per pick:
+// at that size the per-layer GEMM, bias and GELU launches cost far more
+// than the arithmetic.  One launch does it all: CTA (m, t) runs model m on
+// rows [16t, 16t + 16) through every layer, with the activations in shared
+// memory (bf16, as the layered path rounds them), warp-level bf16 tensor-core
+// tiles (mma m16n8k16, fp32 accumulation) whose B operands stream straight
+// from the model's bf16 weights in L2, and bias + GELU fused into the tile
+// epilogue.  The models of one row tile form a thread-block cluster; once
+// every model's output tile is in its CTA's shared memory, CTA 0 of the
+// cluster reads them through distributed shared memory and writes their
+// mean, summed in model order (deterministic).
+constexpr int kEnsMaxModels = 8;  // portable cluster size
+constexpr int kEnsH = 256;        // hidden width the fused kernel is built for
+constexpr int kEnsMaxOut = 256;
+constexpr int kEnsThreads = 256;
+
+struct EnsModel {
+    const bf16* wb;   // bf16 weights (layer l at woff[l], [out][in] row-major)
+    const float* w;   // fp32 arena (biases at boff[l])
+};
+struct EnsArgs {
+    EnsModel m[kEnsMaxModels];
+    long long woff[4], boff[4];
+    int nmodels, din, dout;
+    const float* x;  // [n][din]
+    float* y;        // [n][dout], the mean over the models
+};
+
+__device__ __forceinline__ void mma_bf16_16816(float* d, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One layer for 16 rows: out[16][N] = act[16][K] W^T + bias, then GELU into
+// the next activation buffer (hidden) or fp32 into `outf` (last layer).
+// Warp w computes the n-tiles w, w + 8, ... (8 columns each), up to kNT per
+// pass, sharing each A fragment across them.
+template <int kNT>
+__device__ __forceinline__ void ens_layer(const bf16* __restrict__ act, int lda, int K, const bf16* __restrict__ W,
+                                          const float* __restrict__ bias, int N, bf16* next, int ldn,
+                                          float* outf, int ldo) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int ntiles = N / 8;
+    for (int j0 = warp; j0 < ntiles; j0 += 8 * kNT) {
+        float acc[kNT][4];
+#pragma unroll
+        for (int q = 0; q < kNT; q++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[q][e] = 0.f;
+        for (int k0 = 0; k0 < K; k0 += 16) {
+            uint32_t a[4];
+            a[0] = *(const uint32_t*)(act + g * lda + k0 + 2 * t);
+            a[1] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 2 * t);
+            a[2] = *(const uint32_t*)(act + g * lda + k0 + 8 + 2 * t);
+            a[3] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 8 + 2 * t);
+#pragma unroll
+            for (int q = 0; q < kNT; q++) {
+                const int j = j0 + q * 8;
+                if (j < ntiles) {
+                    const bf16* wr = W + (size_t)(j * 8 + g) * K + k0 + 2 * t;
+                    uint32_t b[2];
+                    b[0] = __ldg((const unsigned int*)wr);
+                    b[1] = __ldg((const unsigned int*)(wr + 8));
+                    mma_bf16_16816(acc[q], a, b);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kNT; q++) {
+            const int j = j0 + q * 8;
+            if (j >= ntiles) continue;
+            const int c = j * 8 + 2 * t;
+            const float b0 = bias[c], b1 = bias[c + 1];
+            const float v[4] = {acc[q][0] + b0, acc[q][1] + b1, acc[q][2] + b0, acc[q][3] + b1};
+            if (next) {
+                *(__nv_bfloat162*)(next + g * ldn + c) = __floats2bfloat162_rn(gelu(v[0]), gelu(v[1]));
+                *(__nv_bfloat162*)(next + (g + 8) * ldn + c) = __floats2bfloat162_rn(gelu(v[2]), gelu(v[3]));
+            } else {
+                outf[g * ldo + c] = v[0];
+                outf[g * ldo + c + 1] = v[1];
+                outf[(g + 8) * ldo + c] = v[2];
+                outf[(g + 8) * ldo + c + 1] = v[3];
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kEnsThreads) k_mlp_ensemble(EnsArgs a) {
+    namespace cg = cooperative_groups;
+    constexpr int kLd = kEnsH + 8;  // padded rows: fragment loads spread over banks
+    __shared__ __align__(16) bf16 s_act[2][16 * kLd];
+    __shared__ __align__(16) float s_out[16 * kEnsMaxOut];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int model = (int)cluster.block_rank();
+    const int row0 = blockIdx.y * 16;
+    const EnsModel M = a.m[model];
+    for (int i = threadIdx.x; i < 16 * a.din; i += kEnsThreads) {
+        const int r = i / a.din, k = i % a.din;
+        s_act[0][r * kLd + k] = __float2bfloat16(a.x[(size_t)(row0 + r) * a.din + k]);
+    }
+    __syncthreads();
+    const int dims[5] = {a.din, kEnsH, kEnsH, kEnsH, a.dout};
+    for (int l = 0; l < 4; l++) {
+        const bf16* in = s_act[l & 1];
+        bf16* nxt = l < 3 ? s_act[(l + 1) & 1] : nullptr;
+        ens_layer<4>(in, kLd, dims[l], M.wb + a.woff[l], M.w + a.boff[l], dims[l + 1], nxt, kLd, s_out, a.dout);
+        __syncthreads();
+    }
+    cluster.sync();
+    if (model == 0) {
+        const float inv = 1.0f / (float)a.nmodels;
+        for (int i = threadIdx.x; i < 16 * a.dout; i += kEnsThreads) {
+            float sum = 0.f;
+            for (int m = 0; m < a.nmodels; m++) sum += cluster.map_shared_rank(s_out, m)[i];
+            a.y[(size_t)(row0 + i / a.dout) * a.dout + i % a.dout] = sum * inv;
+        }
+    }
+    cluster.sync();  // keep every CTA's shared memory alive until CTA 0 has read it
+}
 
 }  // namespace
 
@@ -394,6 +520,62 @@ int bine_mlp_train_step(bine_mlp_t mlp, const float* d_x, const float* d_t, cons
         MLP_TRY(cudaStreamSynchronize(s));
     }
     MLP_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
+struct bine_mlp_ensemble_s {
+    std::vector<bine_mlp_t> models;
+};
+
+int bine_mlp_ensemble_create(const bine_mlp_t* models, int nmodels, bine_mlp_ensemble_t* out) {
+    if (!out || !models || nmodels < 1 || nmodels > kEnsMaxModels)
+        return mfail(BINE_ERR_ARG, "an ensemble holds 1 to 8 models");
+    *out = nullptr;
+    const bine_mlp_t m0 = models[0];
+    if (!m0) return mfail(BINE_ERR_ARG, "null model");
+    if (m0->h != kEnsH || m0->din > kEnsH || m0->dout > kEnsMaxOut)
+        return mfail(BINE_ERR_ARG, "the fused forward takes hidden width 256, input and output widths up to 256");
+    for (int i = 1; i < nmodels; i++)
+        if (!models[i] || models[i]->din != m0->din || models[i]->h != m0->h || models[i]->dout != m0->dout)
+            return mfail(BINE_ERR_ARG, "the models of an ensemble must have the same shape");
+    auto e = new bine_mlp_ensemble_s();
+    e->models.assign(models, models + nmodels);
+    *out = e;
+    return BINE_SUCCESS;
+}
+
+int bine_mlp_ensemble_destroy(bine_mlp_ensemble_t e) {
+    delete e;
+    return BINE_SUCCESS;
+}
+
+int bine_mlp_ensemble_forward(bine_mlp_ensemble_t e, const float* d_x, int n, float* d_y, void* stream) {
+    if (!e || !d_x || !d_y || n <= 0 || n % 16) return mfail(BINE_ERR_ARG, "batch must be a positive multiple of 16");
+    if (n / 16 > 65535) return mfail(BINE_ERR_ARG, "batch too large for one launch");
+    EnsArgs a{};
+    const bine_mlp_t m0 = e->models[0];
+    for (int l = 0; l < 4; l++) {
+        a.woff[l] = (long long)m0->woff[l];
+        a.boff[l] = (long long)m0->boff[l];
+    }
+    a.nmodels = (int)e->models.size();
+    for (int i = 0; i < a.nmodels; i++) a.m[i] = EnsModel{e->models[i]->wb, e->models[i]->w};
+    a.din = m0->din;
+    a.dout = m0->dout;
+    a.x = d_x;
+    a.y = d_y;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)a.nmodels, (unsigned)(n / 16), 1);
+    cfg.blockDim = dim3(kEnsThreads, 1, 1);
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)a.nmodels;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MLP_TRY(cudaLaunchKernelEx(&cfg, k_mlp_ensemble, a));
     return BINE_SUCCESS;
 }
 

@@ -414,19 +414,20 @@ def train(X, Y, M, steps=3000, batch=256, lr=1e-3, seed=0, log=None, val=None, c
 
 def predict(mlp, X):
     """Model outputs [n, OUT_DIM] (standardised log2 time, log2 link bytes);
-    for a list of models (an ensemble), the mean of their outputs."""
+    for a list of models (an ensemble), the mean of their outputs.  One
+    fused launch (bine_mlp_ensemble_forward) per call."""
     import torch
 
-    if isinstance(mlp, (list, tuple)):
-        return np.mean([predict(m, X) for m in mlp], axis=0)
+    import bine_trees_fugaku_b200 as bine
+
+    ens = mlp if isinstance(mlp, bine.Ensemble) else bine.Ensemble(mlp if isinstance(mlp, (list, tuple)) else [mlp])
     n = X.shape[0]
     pad = (-n) % 16
     Xp = np.concatenate([X, np.zeros((pad, IN_DIM), np.float32)]) if pad else X
-    out = []
-    bs = mlp.max_batch
-    for lo in range(0, Xp.shape[0], bs):
-        out.append(mlp.forward(torch.from_numpy(Xp[lo:lo + bs]).cuda()).cpu().numpy())
-    return np.concatenate(out)[:n]
+    out = ens.forward(torch.from_numpy(np.ascontiguousarray(Xp, np.float32)).cuda()).cpu().numpy()
+    if ens is not mlp:
+        ens.close()
+    return out[:n]
 
 
 def evaluate(pred, T, Lb, valid, configs, shortlist=3):
@@ -520,11 +521,12 @@ class Picker:
             if [tuple(a) for a in arms] != ARMS or dims != (IN_DIM, 256, OUT_DIM) or \
                     meta.get("feature_version") != FEATURE_VERSION:
                 raise ValueError(f"{path}: arm space, features or model shape differ from this build")
-            self.mlp = []
+            self.models = []
             for row in p:  # an ensemble: predictions are averaged
                 m = bine.MLP(dims[0], dims[1], dims[2], 16, seed=0)
                 m.set_params(row)
-                self.mlp.append(m)
+                self.models.append(m)
+            self.mlp = bine.Ensemble(self.models)
 
     def ranking(self, coll, P, count, es, dims=None, keep=None):
         """Candidate arm indices, best first.  keep = (variant, ports)

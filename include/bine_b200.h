@@ -338,6 +338,17 @@ int bine_mlp_train_step(bine_mlp_t mlp, const float *d_x, const float *d_t, cons
                         void *stream, float *loss);
 const char *bine_mlp_last_error(void);
 
+/* Inference of an ensemble of 1..8 models of the same shape (hidden width
+ * 256, input and output widths up to 256) in ONE launch: d_y [n x out]
+ * receives the mean of the models' outputs, summed in model order.  The
+ * picker ranks the arms of one call with it (a 16-row batch).  The
+ * ensemble refers to the models' current weights; it holds no copy.  Not in
+ * the reference. */
+typedef struct bine_mlp_ensemble_s *bine_mlp_ensemble_t;
+int bine_mlp_ensemble_create(const bine_mlp_t *models, int nmodels, bine_mlp_ensemble_t *ens);
+int bine_mlp_ensemble_forward(bine_mlp_ensemble_t ens, const float *d_x, int n, float *d_y, void *stream);
+int bine_mlp_ensemble_destroy(bine_mlp_ensemble_t ens);
+
 /* ------------------------------------------------------ schedule queries
  * Host-only: these plan the call with the communicator's current settings
  * and need no GPU.  `count` and `root` have the meaning of the collective's

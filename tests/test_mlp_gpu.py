@@ -49,3 +49,31 @@ def test_training_lowers_the_loss():
         last = m.train_step(xd, td, md, 1e-3)
     assert last < 0.2 * first
     m.close()
+
+
+@pytest.mark.parametrize("nmodels,din,dout,n", [(5, 16, 144, 16), (1, 32, 64, 48), (8, 16, 256, 32), (3, 256, 16, 16)])
+def test_fused_ensemble_forward_matches_the_reference_and_the_layered_path(nmodels, din, dout, n):
+    """bine_mlp_ensemble_forward (one launch for every model and layer)
+    against the CPU reference's mean over the models, and against the
+    layered per-model path: the same bf16 rounding points, fp32 sums in
+    another order."""
+    rng = np.random.default_rng(nmodels * 100 + din)
+    models = [bine.MLP(din, 256, dout, 64, seed=s) for s in range(nmodels)]
+    for m in models:  # nonzero biases exercise the fused epilogue
+        p = m.get_params()
+        for w, b, nout, nin in m.layout():
+            p[b:b + nout] = rng.standard_normal(nout).astype(np.float32) * 0.1
+        m.set_params(p)
+    x = rng.standard_normal((n, din)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    ens = bine.Ensemble(models)
+    y = ens.forward(xd).cpu().numpy()
+    ref = np.mean([mlp_ref.forward(m.get_params(), m.layout(), x)[0][-1] for m in models], axis=0)
+    assert np.abs(y - ref).max() <= 2e-2 * np.abs(ref).max()
+    layered = np.mean([m.forward(xd).cpu().numpy() for m in models], axis=0)
+    assert np.abs(y - layered).max() <= 2e-2 * np.abs(layered).max()
+    # Deterministic: the models' outputs are summed in model order.
+    assert np.array_equal(ens.forward(xd).cpu().numpy(), y)
+    ens.close()
+    for m in models:
+        m.close()
