@@ -1949,9 +1949,9 @@ int bine_plan_verify(bine_comm_t comm, bine_coll_t coll, long count, int root) {
     std::shared_ptr<Schedule> s;
     int rc = plan_for_query(comm, coll, count, root, &s);
     if (rc) return rc;
-    std::string err;
-    if (!comm->planner->verify(make_key(comm, coll, count, root), *s, &err)) return fail(BINE_ERR_UNSUPPORTED, err);
-    return BINE_SUCCESS;
+    // The communicator's proof cache, as the engine itself consults before
+    // running a schedule.
+    return verify_cached(comm, make_key(comm, coll, count, root), *s);
 }
 
 int bine_plan_stats(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t out[5]) {
