@@ -1122,7 +1122,8 @@ def run_picker_suite(args):
         configs = pk.sample_configs(args.picker_n, seed=args.picker_seed)
         c2, _, T2, L2, v2 = pk.measure(configs, reps=3, time_budget_s=args.picker_budget, log=log)
         perm = np.random.default_rng(5 + args.picker_seed).permutation(len(c2))
-        te.extend(int(i) + len(cfgs) for i in np.sort(perm[: len(c2) // 5]))
+        n_hold = len(c2) // 5 if args.picker_holdout is None else min(args.picker_holdout, len(c2) // 2)
+        te.extend(int(i) + len(cfgs) for i in np.sort(perm[:n_hold]))
         cfgs += c2
         T.append(T2)
         Lb.append(L2)
@@ -1130,8 +1131,8 @@ def run_picker_suite(args):
     T, Lb, valid = np.concatenate(T), np.concatenate(Lb), np.concatenate(valid)
     te = np.array(sorted(te), np.int64)
     X = np.array([pk.features(c["coll"], c["P"], c["count"], c["es"], c["dims"]) for c in cfgs], np.float32)
-    np.savez_compressed(os.path.join(out_dir, "picker_dataset.npz"), X=X, T=T.astype(np.float32), Lb=Lb,
-                        valid=valid, test=te, configs=json.dumps(cfgs))
+    np.savez_compressed(os.path.join(out_dir, "picker_dataset.npz"), X=X, T=T.astype(np.float32),
+                        Lb=Lb.astype(np.float32), valid=valid, test=te, configs=json.dumps(cfgs))
     t_measure = time.time() - t0
     # Noise ceiling: re-time some held-out calls; how often is the first
     # measurement's best arm within 5 % of the second measurement's best?
@@ -1142,7 +1143,7 @@ def run_picker_suite(args):
         assert c2 == [cfgs[i] for i in sub]
         hits = rows = 0
         for k, i in enumerate(sub):
-            both = valid[i] & v2[k]
+            both = valid[i] & v2[k] & pk.allowed_arms(cfgs[i], valid[i])
             if not both.any():
                 continue
             rows += 1
@@ -1200,6 +1201,8 @@ def run_picker_suite(args):
     line = {"suite": "picker", "metric": "learned pick vs exhaustive search (held-out calls)",
             **ev, "models": len(mlps), "single_model_pick_within_5pct": single["pick_within_5pct_of_optimum"],
             "noise_ceiling": ceiling, "calls_measured": len(cfgs), "arms": pk.NARMS,
+            "training_calls": int(len(tr)), "training_samples": int(valid[tr].sum()),
+            "validation_calls": int(len(va)),
             "valid_arms_per_call_mean": float(valid.sum(1).mean()) if len(cfgs) else 0.0,
             "train_loss_first_last": [losses[0], float(np.mean(losses[-50:]))],
             "measure_s": t_measure, "train_s": t_train,
@@ -1210,8 +1213,11 @@ def run_picker_suite(args):
             "config": {"model": "ensemble of bine_mlp 16-256-256-256-%d GELU, bf16 weights, fp32 accumulate" % pk.OUT_DIM,
                        "engine": "steps", "timing": "per arm: median of 3 CUDA-event batches of back-to-back "
                                                     "launches (each batch ~300 us, at most 32 launches)",
-                       "calls": "sampled: 60% allreduce / 20% reduce_scatter / 20% allgather, P on [4, 4096], "
-                                "per-rank message log-uniform 32 B..256 MiB (P x message <= 2 GiB)"}}
+                       "calls": "sampled: 60% allreduce / 20% reduce_scatter / 20% allgather, P on [4, 4096] "
+                                "([4, 2048] for reduce_scatter and allgather), per-rank message log-uniform "
+                                "32 B..256 MiB (P x message <= 2 GiB)",
+                       "samples": "one (call, arm) timing per training sample; held-out calls are judged "
+                                  "against exhaustive search over every valid arm"}}
     print(json.dumps(line))
     return 0
 
@@ -1248,6 +1254,8 @@ def main():
     ap.add_argument("--picker-data", default=None,
                     help="measured picker_dataset.npz files to train on (comma-separated; --picker-n 0 to measure none)")
     ap.add_argument("--picker-repeat", type=int, default=150, help="held-out calls re-timed for the noise ceiling")
+    ap.add_argument("--picker-holdout", type=int, default=None,
+                    help="held-out calls among the newly measured ones (default: a fifth)")
     ap.add_argument("--out", default=None, help="directory for the picker's dataset and weights")
     args = ap.parse_args()
     configure(args)

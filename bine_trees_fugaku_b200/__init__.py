@@ -109,6 +109,9 @@ def lib():
         "bine_comm_set_algo": [vp, i, i, i, i],
         "bine_comm_set_engine": [vp, i],
         "bine_comm_set_segment": [vp, ctypes.c_longlong],
+        "bine_comm_set_fusion": [vp, i],
+        "bine_plan_fused": [vp, i, ctypes.c_long, i, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz),
+                            i64p, sz, ctypes.POINTER(sz), i64p],
         "bine_comm_set_float_order": [vp, i],
         "bine_comm_set_step_timeout": [vp, ctypes.c_uint],
         "bine_debug_set_barrier_extra": [vp, ctypes.c_uint],
@@ -217,9 +220,11 @@ class Comm:
         # Settings as last set (the picker reads them): per-collective
         # variant (None: the reference's default), ports, engine, float order.
         self.algo = {}
+        self.family = {}
         self.ports = 1
         self.engine = "fused"
         self.float_order = "reference"
+        self.fusion = 1
 
     def close(self):
         if getattr(self, "_h", None):
@@ -249,6 +254,7 @@ class Comm:
         check(lib().bine_comm_set_algo(self._h, COLL_ID[coll], VARIANTS[coll][variant], FAMILY[family],
                                        DISTANCE[distance]))
         self.algo[coll] = variant
+        self.family[coll] = family
 
     def set_engine(self, engine):
         check(lib().bine_comm_set_engine(self._h, {"fused": ENGINE_FUSED, "steps": ENGINE_STEPS,
@@ -257,6 +263,12 @@ class Comm:
 
     def set_segment(self, segment_bytes):
         check(lib().bine_comm_set_segment(self._h, segment_bytes))
+
+    def set_fusion(self, levels):
+        """Levels of the reference's schedule per pass of the PIPELINED
+        engine (1: every level on its own)."""
+        check(lib().bine_comm_set_fusion(self._h, levels))
+        self.fusion = levels
 
     def set_float_order(self, order):
         check(lib().bine_comm_set_float_order(self._h, {"reference": ORDER_REFERENCE, "fast": ORDER_FAST}.get(order, order)))
@@ -398,6 +410,23 @@ class Comm:
                                    items.ctypes.data_as(i32p), nit.value, ctypes.byref(nit),
                                    deps.ctypes.data_as(i32p), ndp.value, ctypes.byref(ndp)))
         return pieces[: npc.value], items[: nit.value], deps[: ndp.value]
+
+    def plan_fused(self, coll, count, root=0, levels=3):
+        """Fused form of the call's schedule: (moves [n, 6] = (pass, elements,
+        first leaf, leaves, first destination, destinations), leaves [n, 4] =
+        (rank, buffer, additions, offset), destinations [n, 3] = (rank,
+        buffer, offset), workspace elements per rank)."""
+        nm, nl, nd, tmp = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_int64()
+        check(lib().bine_plan_fused(self._h, COLL_ID[coll], count, root, levels, None, 0, ctypes.byref(nm), None, 0,
+                                    ctypes.byref(nl), None, 0, ctypes.byref(nd), ctypes.byref(tmp)))
+        mv = np.zeros((max(1, nm.value), 6), np.int64)
+        lv = np.zeros((max(1, nl.value), 4), np.int64)
+        dv = np.zeros((max(1, nd.value), 3), np.int64)
+        p64 = ctypes.POINTER(ctypes.c_int64)
+        check(lib().bine_plan_fused(self._h, COLL_ID[coll], count, root, levels, mv.ctypes.data_as(p64), nm.value,
+                                    ctypes.byref(nm), lv.ctypes.data_as(p64), nl.value, ctypes.byref(nl),
+                                    dv.ctypes.data_as(p64), nd.value, ctypes.byref(nd), None))
+        return mv[:nm.value], lv[:nl.value], dv[:nd.value], tmp.value
 
     def plan_messages(self, coll, count, root=0):
         n = ctypes.c_size_t(0)

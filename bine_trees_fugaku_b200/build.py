@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libbine_b200.so")
 
-SOURCES = ["bine_capi.cu", "bine_plan.cc", "bine_mlp.cu"]
+SOURCES = ["bine_capi.cu", "bine_plan.cc", "bine_mlp.cu", "bine_fuse.cc"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

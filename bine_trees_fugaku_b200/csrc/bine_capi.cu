@@ -95,6 +95,25 @@ struct DevSteps {
     }
 };
 
+// Device tables of a fused schedule (level fusion) and its dataflow plan.
+struct DevFused {
+    dev::FusedMoveDev* moves = nullptr;
+    dev::FusedLeafDev* leaves = nullptr;
+    dev::FusedDstDev* dsts = nullptr;
+    DevFlow flow;
+    int64_t tmp_elems = 0;
+    int npasses = 0;
+    ~DevFused() {
+        cudaFree(moves);
+        cudaFree(leaves);
+        cudaFree(dsts);
+    }
+};
+static_assert(sizeof(FusedMove) == sizeof(dev::FusedMoveDev), "fused move layouts differ");
+static_assert(sizeof(FusedLeaf) == sizeof(dev::FusedLeafDev), "fused leaf layouts differ");
+static_assert(sizeof(FusedDst) == sizeof(dev::FusedDstDev), "fused destination layouts differ");
+static_assert(dev::kFuseLeaves == kFuseMaxLeaves && dev::kFuseDsts == kFuseMaxDsts, "fusion bounds differ");
+
 // Device copy of the exact reduction trees of one call.
 struct DevTrees {
     dev::TreeSeg* segs = nullptr;
@@ -168,6 +187,15 @@ struct PlanKeyEsHash {
     }
 };
 
+struct FusedKey {
+    PlanKeyEs base;
+    int levels;
+    bool operator==(const FusedKey& o) const { return base == o.base && levels == o.levels; }
+};
+struct FusedKeyHash {
+    size_t operator()(const FusedKey& x) const { return PlanKeyEsHash()(x.base) * 131 + (size_t)x.levels; }
+};
+
 // A schedule's routing does not depend on `count` once every block is
 // non-empty, so one symbolic proof covers every count of the same
 // structure (collective, variant, family, distance, ports, root) and
@@ -201,6 +229,8 @@ struct bine_comm_s {
     std::unordered_map<PlanKey, std::shared_ptr<Schedule>, PlanKeyHash> schedules;
     std::unordered_map<PlanKeyEs, std::shared_ptr<DevSteps>, PlanKeyEsHash> dev_steps;
     std::unordered_map<PlanKeyEs, std::shared_ptr<DevTrees>, PlanKeyEsHash> dev_trees;
+    std::unordered_map<FusedKey, std::shared_ptr<DevFused>, FusedKeyHash> dev_fused;
+    int fusion = 1;  // levels per pass of the PIPELINED engine (1: every level on its own)
     std::unordered_map<StructKey, int, StructKeyHash> verified;  // 1: proven, 0: refuted
     std::unordered_map<StructKey, std::string, StructKeyHash> refuted_why;
     long long segment_bytes = 0;
@@ -480,6 +510,107 @@ int get_dev_flow(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevSte
     CUDA_TRY(cudaMemset(f->ctl, 0, (3 + f->nlevels) * sizeof(unsigned)));
     (*steps)->flow = f;
     *out = f;
+    return BINE_SUCCESS;
+}
+
+// Ranks whose receive row is a result of the collective.
+std::vector<bool> result_rows(const PlanKey& k, int P) {
+    std::vector<bool> rows(P, true);
+    if (k.coll == kReduce || k.coll == kGather) {
+        rows.assign(P, false);
+        rows[k.root] = true;
+    }
+    return rows;
+}
+
+int fused_schedule(bine_comm_t c, const PlanKey& k, int levels, std::shared_ptr<Schedule>* s, FusedSchedule* fs) {
+    int rc = get_schedule(c, k, s);
+    if (rc) return rc;
+    rc = verify_cached(c, k, **s);
+    if (rc) return rc;
+    std::string err;
+    if (!fuse_schedule(**s, c->P, levels, result_rows(k, c->P), fs, &err)) return fail(BINE_ERR_INTERNAL, err);
+    return BINE_SUCCESS;
+}
+
+int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFused>* out) {
+    const FusedKey key{PlanKeyEs{k, es, c->segment_bytes}, c->fusion};
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        auto it = c->dev_fused.find(key);
+        if (it != c->dev_fused.end()) {
+            *out = it->second;
+            return BINE_SUCCESS;
+        }
+    }
+    std::shared_ptr<Schedule> s;
+    FusedSchedule fs;
+    int rc = fused_schedule(c, k, c->fusion, &s, &fs);
+    if (rc) return rc;
+    // Every row range the kernel will touch must lie inside its row.
+    const int64_t rows[3] = {s->send_elems, s->recv_elems, fs.tmp_elems};
+    for (const auto& pass : fs.passes)
+        for (const FusedMove& m : pass) {
+            if (m.n < 0 || m.nleaves < 1 || m.nleaves > kFuseMaxLeaves || m.ndst < 1 || m.ndst > kFuseMaxDsts)
+                return fail(BINE_ERR_INTERNAL, "fusion produced a move outside the kernel's bounds");
+            int depth = 0, maxd = 0;
+            for (int j = 0; j < m.nleaves; j++) {
+                const FusedLeaf& lf = fs.leaves[m.leaf_begin + j];
+                if (lf.rank < 0 || lf.rank >= c->P || lf.buf > kBufTmp || lf.off < 0 || lf.off + m.n > rows[lf.buf] ||
+                    (j == 0 && lf.adds != 0) || lf.adds > 3)
+                    return fail(BINE_ERR_INTERNAL, "fusion produced a leaf outside its buffer row");
+                depth += 1 - lf.adds;
+                maxd = std::max(maxd, depth);
+                if (depth < 1) return fail(BINE_ERR_INTERNAL, "fusion produced a malformed program");
+            }
+            if (depth != 1 || maxd > kFuseMaxDepth) return fail(BINE_ERR_INTERNAL, "fusion produced a malformed program");
+            for (int j = 0; j < m.ndst; j++) {
+                const FusedDst& d = fs.dsts[m.dst_begin + j];
+                if (d.rank < 0 || d.rank >= c->P || d.buf > kBufTmp || d.buf == kBufSend || d.off < 0 ||
+                    d.off + m.n > rows[d.buf])
+                    return fail(BINE_ERR_INTERNAL, "fusion produced a destination outside its buffer row");
+            }
+        }
+    FlowPlan fp;
+    const int64_t piece = c->segment_bytes > 0 ? std::max<int64_t>(16, c->segment_bytes / es) : 0;
+    build_flow_fused(fs, c->P, piece, std::max<int64_t>(1, 4096 / es), kFlowMaxItemBytes / es,
+                     kFlowItemsPerSm * c->num_sms, dev::kFusedPieces, &fp);
+    auto d = std::make_shared<DevFused>();
+    d->tmp_elems = fs.tmp_elems;
+    d->npasses = (int)fs.passes.size();
+    std::vector<FusedMove> moves;
+    for (const auto& pass : fs.passes) moves.insert(moves.end(), pass.begin(), pass.end());
+    std::vector<dev::FusedMoveDev> dm(moves.size());
+    if (!dm.empty()) std::memcpy(dm.data(), moves.data(), dm.size() * sizeof(dev::FusedMoveDev));
+    std::vector<dev::FusedLeafDev> dl(fs.leaves.size());
+    if (!dl.empty()) std::memcpy(dl.data(), fs.leaves.data(), dl.size() * sizeof(dev::FusedLeafDev));
+    std::vector<dev::FusedDstDev> dd(fs.dsts.size());
+    if (!dd.empty()) std::memcpy(dd.data(), fs.dsts.data(), dd.size() * sizeof(dev::FusedDstDev));
+    DevFlow& f = d->flow;
+    f.nitems = (int)fp.items.size();
+    f.nlevels = (int)fp.level_items.size();
+    std::vector<dev::StepChunk> pieces(fp.pieces.size());
+    if (!pieces.empty()) std::memcpy(pieces.data(), fp.pieces.data(), pieces.size() * sizeof(dev::StepChunk));
+    std::vector<dev::FlowItem> items(fp.items.size());
+    if (!items.empty()) std::memcpy(items.data(), fp.items.data(), items.size() * sizeof(dev::FlowItem));
+    cudaError_t e[7];
+    fill(&d->moves, dm, &e[0]);
+    fill(&d->leaves, dl, &e[1]);
+    fill(&d->dsts, dd, &e[2]);
+    fill(&f.pieces, pieces, &e[3]);
+    fill(&f.items, items, &e[4]);
+    fill(&f.deps, fp.deps, &e[5]);
+    fill(&f.level_items, fp.level_items, &e[6]);
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return fail(BINE_ERR_CUDA, "uploading the fused schedule failed");
+    CUDA_TRY(cudaMalloc(&f.done, std::max(1, f.nitems) * sizeof(unsigned)));
+    CUDA_TRY(cudaMalloc(&f.ctl, (3 + f.nlevels) * sizeof(unsigned)));
+    CUDA_TRY(cudaMemset(f.done, 0, std::max(1, f.nitems) * sizeof(unsigned)));
+    CUDA_TRY(cudaMemset(f.ctl, 0, (3 + f.nlevels) * sizeof(unsigned)));
+    std::lock_guard<std::mutex> lk(c->mu);
+    trim(c->dev_fused, kMaxCachedDeviceTables);
+    c->dev_fused.emplace(key, d);
+    *out = d;
     return BINE_SUCCESS;
 }
 
@@ -1054,6 +1185,43 @@ int launch_flow(bine_comm_t c, const DevSteps& d, const DevFlow& f, const char* 
     return BINE_SUCCESS;
 }
 
+template <typename T>
+int launch_flow_fused(bine_comm_t c, const DevFused& d, const char* send, long long ist, char* recv, long long ost) {
+    const DevFlow& f = d.flow;
+    if (f.nitems == 0) return BINE_SUCCESS;
+    const size_t es = sizeof(T);
+    const size_t tmp_stride = ((size_t)d.tmp_elems * es + 255) / 256 * 256;
+    int rc = ensure_work(c, std::max<size_t>(tmp_stride * c->P, 256));
+    if (rc) return rc;
+    dev::StepBufs B;
+    B.base[kBufSend] = const_cast<char*>(send);
+    B.base[kBufRecv] = recv;
+    B.base[kBufTmp] = c->work;
+    B.stride[kBufSend] = ist;
+    B.stride[kBufRecv] = ost;
+    B.stride[kBufTmp] = (long long)tmp_stride;
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_flow_fused<T>, dev::kFlowThreads, 0));
+    const int blocks = std::max(1, std::min(std::max(1, per_sm) * c->num_sms, f.nitems));
+    dev::k_flow_fused<T><<<blocks, dev::kFlowThreads, 0, c->stream>>>(
+        B, d.moves, d.leaves, d.dsts, f.pieces, f.items, f.nitems, f.deps, f.level_items, f.nlevels, f.done, f.ctl,
+        c->status, c->step_timeout_ns, c->barrier_extra);
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
+int launch_flow_fused_dt(bine_comm_t c, int dt, const DevFused& d, const char* send, long long ist, char* recv,
+                         long long ost) {
+    switch (dt) {
+    case BINE_INT32: return launch_flow_fused<int32_t>(c, d, send, ist, recv, ost);
+    case BINE_INT64: return launch_flow_fused<int64_t>(c, d, send, ist, recv, ost);
+    case BINE_FLOAT: return launch_flow_fused<float>(c, d, send, ist, recv, ost);
+    case BINE_DOUBLE: return launch_flow_fused<double>(c, d, send, ist, recv, ost);
+    case BINE_CHAR: return launch_flow_fused<int8_t>(c, d, send, ist, recv, ost);
+    }
+    return fail(BINE_ERR_ARG, "bad datatype");
+}
+
 int launch_flow_dt(bine_comm_t c, int dt, const DevSteps& d, const DevFlow& f, const char* send, long long ist,
                    char* recv, long long ost) {
     switch (dt) {
@@ -1155,6 +1323,12 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
         rc = get_dev_steps(c, k, es, &d);
         if (rc) return rc;
         return launch_steps_dt(c, dt, *d, in, ist, out, ost);
+    }
+    if (c->engine == BINE_ENGINE_PIPELINED && c->fusion > 1) {
+        std::shared_ptr<DevFused> d;
+        rc = get_dev_fused(c, k, es, &d);
+        if (rc) return rc;
+        return launch_flow_fused_dt(c, dt, *d, in, ist, out, ost);
     }
     if (c->engine == BINE_ENGINE_PIPELINED) {
         std::shared_ptr<DevSteps> d;
@@ -1813,6 +1987,13 @@ int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int fami
     return BINE_SUCCESS;
 }
 
+int bine_comm_set_fusion(bine_comm_t comm, int levels) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if (levels < 1 || levels > 64) return fail(BINE_ERR_ARG, "levels per pass must be in [1, 64]");
+    comm->fusion = levels;
+    return BINE_SUCCESS;
+}
+
 int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     if (segment_bytes < 0) return fail(BINE_ERR_ARG, "segment size must be >= 0");
@@ -2003,7 +2184,17 @@ int bine_plan_flow(bine_comm_t comm, bine_coll_t coll, long count, int root, int
     int rc = plan_for_query(comm, coll, count, root, &s);
     if (rc) return rc;
     FlowPlan fp;
-    flow_plan(*s, comm->P, elem_size, comm->segment_bytes, target_items, &fp);
+    if (comm->fusion > 1) {
+        // The fused plan: pieces index the fused moves in pass order.
+        FusedSchedule fs;
+        rc = fused_schedule(comm, make_key(comm, coll, count, root), comm->fusion, &s, &fs);
+        if (rc) return rc;
+        const int64_t piece = comm->segment_bytes > 0 ? std::max<int64_t>(16, comm->segment_bytes / elem_size) : 0;
+        build_flow_fused(fs, comm->P, piece, std::max<int64_t>(1, 4096 / elem_size), kFlowMaxItemBytes / elem_size,
+                         target_items, dev::kFusedPieces, &fp);
+    } else {
+        flow_plan(*s, comm->P, elem_size, comm->segment_bytes, target_items, &fp);
+    }
     for (size_t i = 0; i < fp.pieces.size() && i < piece_cap && pieces; i++) {
         pieces[3 * i] = fp.pieces[i].move;
         pieces[3 * i + 1] = fp.pieces[i].start;
@@ -2018,6 +2209,52 @@ int bine_plan_flow(bine_comm_t comm, bine_coll_t coll, long count, int root, int
     if (n_pieces) *n_pieces = fp.pieces.size();
     if (n_items) *n_items = fp.items.size();
     if (n_deps) *n_deps = fp.deps.size();
+    return BINE_SUCCESS;
+}
+
+int bine_plan_fused(bine_comm_t comm, bine_coll_t coll, long count, int root, int levels, int64_t* moves,
+                    size_t move_cap, size_t* n_moves, int64_t* leaves, size_t leaf_cap, size_t* n_leaves,
+                    int64_t* dsts, size_t dst_cap, size_t* n_dsts, int64_t* tmp_elems) {
+    if (!comm) return fail(BINE_ERR_ARG, "null communicator");
+    if ((int)coll < 0 || (int)coll >= kNumColls) return fail(BINE_ERR_ARG, "invalid collective");
+    if (count <= 0) return fail(BINE_ERR_ARG, "count must be positive");
+    if (levels < 1 || levels > 64) return fail(BINE_ERR_ARG, "levels per pass must be in [1, 64]");
+    std::shared_ptr<Schedule> s;
+    FusedSchedule fs;
+    int rc = fused_schedule(comm, make_key(comm, coll, count, root), levels, &s, &fs);
+    if (rc) return rc;
+    size_t nm = 0;
+    for (const auto& pass : fs.passes) nm += pass.size();
+    if (n_moves) *n_moves = nm;
+    if (n_leaves) *n_leaves = fs.leaves.size();
+    if (n_dsts) *n_dsts = fs.dsts.size();
+    if (tmp_elems) *tmp_elems = fs.tmp_elems;
+    if (moves && move_cap >= nm) {
+        size_t i = 0;
+        for (size_t p = 0; p < fs.passes.size(); p++)
+            for (const FusedMove& m : fs.passes[p]) {
+                int64_t* o = moves + 6 * i++;
+                o[0] = (int64_t)p;
+                o[1] = m.n;
+                o[2] = m.leaf_begin;
+                o[3] = m.nleaves;
+                o[4] = m.dst_begin;
+                o[5] = m.ndst;
+            }
+    }
+    if (leaves && leaf_cap >= fs.leaves.size())
+        for (size_t i = 0; i < fs.leaves.size(); i++) {
+            leaves[4 * i] = fs.leaves[i].rank;
+            leaves[4 * i + 1] = fs.leaves[i].buf;
+            leaves[4 * i + 2] = fs.leaves[i].adds;
+            leaves[4 * i + 3] = fs.leaves[i].off;
+        }
+    if (dsts && dst_cap >= fs.dsts.size())
+        for (size_t i = 0; i < fs.dsts.size(); i++) {
+            dsts[3 * i] = fs.dsts[i].rank;
+            dsts[3 * i + 1] = fs.dsts[i].buf;
+            dsts[3 * i + 2] = fs.dsts[i].off;
+        }
     return BINE_SUCCESS;
 }
 

@@ -975,6 +975,201 @@ __global__ void __launch_bounds__(kFlowThreads, kFlowBlocksPerSm) k_flow(StepBuf
     }
 }
 
+// ------------------------------------------- pipelined engine, fused passes
+// The same dataflow driver as k_flow over a fused schedule (level fusion,
+// bine_plan.h): a piece belongs to a fused move whose value is a postfix
+// program over at most kFuseLeaves state elements, written to at most
+// kFuseDsts destinations.  Each unit (a 16-byte vector, or an element at a
+// piece's unaligned head and tail) loads all of its leaves, evaluates the
+// program on a four-entry register stack in the order of the original
+// levels' additions, and stores the value to every destination; the loads
+// come before the stores, so a move may update its own elements in place.
+struct FusedMoveDev {
+    int64_t n;
+    int32_t leaf_begin, nleaves, dst_begin, ndst;
+};
+struct FusedLeafDev {
+    int32_t rank;
+    uint8_t buf, adds, pad[2];
+    int64_t off;
+};
+struct FusedDstDev {
+    int32_t rank;
+    uint8_t buf, pad[3];
+    int64_t off;
+};
+constexpr int kFuseLeaves = 8;
+constexpr int kFuseDsts = 8;
+constexpr int kFusedPieces = 64;  // pieces per item
+
+// Postfix evaluation on a shift-register stack (s0 is the top): a leaf
+// pushes, each addition pops the top two and pushes their sum.  IEEE and
+// wrapping integer addition are commutative, so only the tree's shape
+// matters, and it is the program's.
+template <typename V, typename Add>
+__device__ __forceinline__ V fused_eval(const V* v, const unsigned char* adds, int nl, Add add) {
+    V s0 = v[0], s1 = v[0], s2 = v[0], s3 = v[0];
+#pragma unroll
+    for (int j = 1; j < kFuseLeaves; j++) {
+        if (j < nl) {
+            s3 = s2;
+            s2 = s1;
+            s1 = s0;
+            s0 = v[j];
+            const int na = adds[j];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                if (a < na) {
+                    s0 = add(s1, s0);
+                    s1 = s2;
+                    s2 = s3;
+                }
+        }
+    }
+    return s0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kFlowThreads) k_flow_fused(StepBufs B, const FusedMoveDev* __restrict__ moves,
+                                                            const FusedLeafDev* __restrict__ leaves,
+                                                            const FusedDstDev* __restrict__ dsts,
+                                                            const StepChunk* __restrict__ pieces,
+                                                            const FlowItem* __restrict__ items, int nitems,
+                                                            const int* __restrict__ deps,
+                                                            const int* __restrict__ level_items, int nlevels,
+                                                            unsigned* done, unsigned* ctl, int* status,
+                                                            unsigned long long timeout_ns, unsigned extra) {
+    __shared__ long long s_pref[kFusedPieces + 1];
+    __shared__ const char* s_leaf[kFusedPieces][kFuseLeaves];
+    __shared__ char* s_dst[kFusedPieces][kFuseDsts];
+    __shared__ unsigned char s_adds[kFusedPieces][kFuseLeaves];
+    __shared__ long long s_nvec[kFusedPieces];
+    __shared__ unsigned char s_head[kFusedPieces], s_nl[kFusedPieces], s_nd[kFusedPieces];
+    __shared__ long long s_warp[kFlowThreads / 32];
+    __shared__ int s_item, s_ok;
+    __shared__ unsigned s_target;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        const unsigned t = ld_acquire(&ctl[2]) + 1u;
+        s_target = t == 0 ? 1u : t;
+    }
+    __syncthreads();
+    const unsigned target = s_target;
+    constexpr long long es = sizeof(T);
+    for (;;) {
+        if (tid == 0) s_item = *(volatile int*)status == kStepOk ? (int)atomicAdd(&ctl[0], 1u) : nitems;
+        __syncthreads();
+        const int i = s_item;
+        if (i >= nitems) break;
+        const FlowItem it = items[i];
+        const int np = it.pend - it.pbeg;  // at most kFusedPieces (the planner's bound)
+        long long units = 0;
+        if (tid < np) {
+            const StepChunk ch = pieces[it.pbeg + tid];
+            const FusedMoveDev m = moves[ch.move];
+            uintptr_t mis = 0, first = 0;
+            for (int j = 0; j < m.nleaves; j++) {
+                const FusedLeafDev lf = leaves[m.leaf_begin + j];
+                const char* a = B.base[lf.buf] + (long long)lf.rank * B.stride[lf.buf] + (lf.off + ch.start) * es;
+                s_leaf[tid][j] = a;
+                s_adds[tid][j] = lf.adds;
+                if (j == 0) first = (uintptr_t)a;
+                mis |= (uintptr_t)a ^ first;
+            }
+            for (int j = 0; j < m.ndst; j++) {
+                const FusedDstDev d = dsts[m.dst_begin + j];
+                char* p = B.base[d.buf] + (long long)d.rank * B.stride[d.buf] + (d.off + ch.start) * es;
+                s_dst[tid][j] = p;
+                mis |= (uintptr_t)p ^ first;
+            }
+            const long long n = ch.n;
+            long long head = n, nvec = 0;
+            if ((mis & 15) == 0) {
+                head = min((long long)((16 - (first & 15)) & 15) / es, n);
+                nvec = (n - head) * es / 16;
+            }
+            units = n - nvec * (16 / es) + nvec;
+            s_nvec[tid] = nvec;
+            s_head[tid] = (unsigned char)min(head, 255ll);
+            s_nl[tid] = (unsigned char)m.nleaves;
+            s_nd[tid] = (unsigned char)m.ndst;
+        }
+        long long inc = units;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        long long before = 0;
+        for (int w = 0; w < warp; w++) before += s_warp[w];
+        if (tid < kFusedPieces) s_pref[tid + 1] = before + inc;
+        if (tid == 0) s_pref[0] = 0;
+        if (warp == 0) {
+            bool ok = true;
+            for (int d = it.dbeg + lane; d < it.dend && ok; d += 32)
+                ok = flow_wait(deps[d], done, ctl, level_items, target, extra, status, timeout_ns);
+            ok = __all_sync(0xffffffffu, ok);
+            if (lane == 0) s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        const long long total = s_pref[np];
+        int cur = 0;
+        for (long long u = tid; u < total; u += kFlowThreads) {
+            if (!(u >= s_pref[cur] && u < s_pref[cur + 1])) {
+                int lo = 0, hi = np - 1;  // last piece starting at or before u
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_pref[mid] <= u) lo = mid; else hi = mid - 1;
+                }
+                cur = lo;
+            }
+            const long long r = u - s_pref[cur];
+            const long long head = s_head[cur], nvec = s_nvec[cur];
+            const int nl = s_nl[cur], nd = s_nd[cur];
+            if (r >= head && r < head + nvec) {
+                const long long off = head * es + (r - head) * 16;
+                uint4 v[kFuseLeaves];
+#pragma unroll
+                for (int j = 0; j < kFuseLeaves; j++)
+                    if (j < nl) v[j] = ld_plain(s_leaf[cur][j] + off);
+                const uint4 val = fused_eval(v, s_adds[cur], nl, [](uint4 x, uint4 y) { return vadd<T>(x, y); });
+#pragma unroll
+                for (int j = 0; j < kFuseDsts; j++)
+                    if (j < nd) *(uint4*)(s_dst[cur][j] + off) = val;
+            } else {
+                const long long e = r < head ? r : r - nvec + nvec * (16 / es);
+                T v[kFuseLeaves];
+#pragma unroll
+                for (int j = 0; j < kFuseLeaves; j++)
+                    if (j < nl) v[j] = *((volatile const T*)s_leaf[cur][j] + e);
+                const T val = fused_eval(v, s_adds[cur], nl, [](T x, T y) { return add_exact<T>(x, y); });
+#pragma unroll
+                for (int j = 0; j < kFuseDsts; j++)
+                    if (j < nd) *((T*)s_dst[cur][j] + e) = val;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            st_release(&done[i], target);
+            red_release_add(&ctl[3 + it.level], 1u);
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&ctl[1], 1u) == gridDim.x - 1) {
+            ctl[0] = 0;
+            ctl[1] = 0;
+            for (int l = 0; l < nlevels; l++) ctl[3 + l] = 0;
+            __threadfence();
+            st_release(&ctl[2], target);
+        }
+    }
+}
+
 }  // namespace dev
 }  // namespace bine
 

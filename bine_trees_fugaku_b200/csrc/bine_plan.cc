@@ -2008,10 +2008,14 @@ struct FlowAccess {
     bool write;
 };
 
-}  // namespace
-
-void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
-                int target_items, int max_pieces, FlowPlan* out) {
+// The shared core of build_flow and build_flow_fused: `sizes[l]` are the
+// element counts of level l's moves (numbered in level order), and
+// visit(move, start, n, fn) calls fn(rank, buf, offset, n, write) for every
+// row range the elements [start, start + n) of that move read or write.
+template <typename Visit>
+void build_flow_impl(const std::vector<std::vector<int64_t>>& sizes, int P, int64_t piece_elems,
+                     int64_t min_item_elems, int64_t max_item_elems, int target_items, int max_pieces, Visit visit,
+                     FlowPlan* out) {
     *out = FlowPlan();
     max_pieces = std::max(1, std::min(max_pieces, kFlowMaxPieces));
     const bool auto_pieces = piece_elems <= 0;
@@ -2019,12 +2023,12 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
     min_item_elems = std::max<int64_t>(1, min_item_elems);
     max_item_elems = std::max(min_item_elems, max_item_elems);
     // Pieces and items, level by level.
-    std::vector<const Move*> move_of;  // level-order move index -> move
+    int32_t nmoves = 0;                // level-order move index
     std::vector<int32_t> level_first;  // first item of each level
-    for (size_t l = 0; l < s.levels.size(); l++) {
+    for (size_t l = 0; l < sizes.size(); l++) {
         level_first.push_back((int32_t)out->items.size());
         int64_t level_elems = 0;
-        for (const Move& m : s.levels[l]) level_elems += m.n;
+        for (int64_t n : sizes[l]) level_elems += n;
         int64_t item_elems = std::max(min_item_elems, (level_elems + target_items - 1) / target_items);
         if (auto_pieces) {
             // Whole multiples of min_item_elems, so that pieces cut from a
@@ -2036,11 +2040,10 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
         }
         int32_t nitems = 0;
         int64_t cur = 0;  // elements in the open item
-        for (const Move& m : s.levels[l]) {
-            const int32_t mi = (int32_t)move_of.size();
-            move_of.push_back(&m);
-            for (int64_t st = 0; st < m.n; st += piece_elems) {
-                const int64_t n = std::min(piece_elems, m.n - st);
+        for (int64_t mn : sizes[l]) {
+            const int32_t mi = nmoves++;
+            for (int64_t st = 0; st < mn; st += piece_elems) {
+                const int64_t n = std::min(piece_elems, mn - st);
                 if (nitems == 0 || cur + n > item_elems ||
                     out->items.back().pend - out->items.back().pbeg >= max_pieces) {
                     const int32_t p = (int32_t)out->pieces.size();
@@ -2071,18 +2074,14 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
         const int32_t i0 = level_first[l], i1 = level_first[l + 1];
         if (i0 == i1) continue;
         touched.clear();
-        auto add = [&](const Region& r, int64_t st, int64_t n, int32_t item, bool write) {
-            const size_t row = (size_t)r.buf * P + r.rank;
-            if (acc[row].empty()) touched.push_back(row);
-            acc[row].push_back(FlowAccess{r.off + st, r.off + st + n, item, write});
-        };
         for (int32_t i = i0; i < i1; i++)
             for (int32_t p = out->items[i].pbeg; p < out->items[i].pend; p++) {
                 const FlowPiece& pc = out->pieces[p];
-                const Move& m = *move_of[pc.move];
-                add(m.a, pc.start, pc.n, i, false);
-                if (m.add) add(m.b, pc.start, pc.n, i, false);
-                add(m.dst, pc.start, pc.n, i, true);
+                visit(pc.move, pc.start, pc.n, [&](int rank, int buf, int64_t off, int64_t n, bool write) {
+                    const size_t row = (size_t)buf * P + rank;
+                    if (acc[row].empty()) touched.push_back(row);
+                    acc[row].push_back(FlowAccess{off, off + n, i, write});
+                });
             }
         cand.assign(i1 - i0, {});
         for (size_t row : touched) {
@@ -2169,6 +2168,51 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
             it.dend = (int32_t)out->deps.size();
         }
     }
+}
+
+}  // namespace
+
+void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
+                int target_items, int max_pieces, FlowPlan* out) {
+    std::vector<std::vector<int64_t>> sizes(s.levels.size());
+    std::vector<const Move*> move_of;
+    for (size_t l = 0; l < s.levels.size(); l++)
+        for (const Move& m : s.levels[l]) {
+            sizes[l].push_back(m.n);
+            move_of.push_back(&m);
+        }
+    build_flow_impl(sizes, P, piece_elems, min_item_elems, max_item_elems, target_items, max_pieces,
+                    [&](int32_t mi, int64_t st, int64_t n, auto fn) {
+                        const Move& m = *move_of[mi];
+                        fn(m.a.rank, m.a.buf, m.a.off + st, n, false);
+                        if (m.add) fn(m.b.rank, m.b.buf, m.b.off + st, n, false);
+                        fn(m.dst.rank, m.dst.buf, m.dst.off + st, n, true);
+                    },
+                    out);
+}
+
+void build_flow_fused(const FusedSchedule& f, int P, int64_t piece_elems, int64_t min_item_elems,
+                      int64_t max_item_elems, int target_items, int max_pieces, FlowPlan* out) {
+    std::vector<std::vector<int64_t>> sizes(f.passes.size());
+    std::vector<const FusedMove*> move_of;
+    for (size_t l = 0; l < f.passes.size(); l++)
+        for (const FusedMove& m : f.passes[l]) {
+            sizes[l].push_back(m.n);
+            move_of.push_back(&m);
+        }
+    build_flow_impl(sizes, P, piece_elems, min_item_elems, max_item_elems, target_items, max_pieces,
+                    [&](int32_t mi, int64_t st, int64_t n, auto fn) {
+                        const FusedMove& m = *move_of[mi];
+                        for (int32_t j = 0; j < m.nleaves; j++) {
+                            const FusedLeaf& lf = f.leaves[m.leaf_begin + j];
+                            fn(lf.rank, lf.buf, lf.off + st, n, false);
+                        }
+                        for (int32_t j = 0; j < m.ndst; j++) {
+                            const FusedDst& d = f.dsts[m.dst_begin + j];
+                            fn(d.rank, d.buf, d.off + st, n, true);
+                        }
+                    },
+                    out);
 }
 
 }  // namespace bine

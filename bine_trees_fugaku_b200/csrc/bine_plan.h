@@ -204,6 +204,63 @@ struct FlowPlan {
 void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_elems, int64_t max_item_elems,
                 int target_items, int max_pieces, FlowPlan* out);
 
+// ------------------------------------------------------- level fusion
+// Fused form of a schedule for the PIPELINED engine.  Consecutive levels
+// are grouped into passes; a pass's moves compute, from the buffer state at
+// the start of the pass, every value the pass leaves behind that a later
+// pass reads or that is part of the result.  A value that the original
+// levels write and read again inside the pass (a partial sum one step
+// passes to the next, a message staged in the workspace) stays in registers
+// and is never written.  Every fused move evaluates a postfix program of
+// leaves (state elements) and writes its value to one or more destinations
+// (a copy that several ranks receive from the same rank in one pass is read
+// once).  The addition trees are those of the original levels, so results
+// are bit-identical; after every pass, every element that is read later or
+// is a result holds what the original levels leave there at that step.
+struct FusedLeaf {  // push state(buf, rank, i + off) for position i, then `adds` additions
+    int32_t rank;
+    uint8_t buf, adds, pad[2];
+    int64_t off;
+};
+struct FusedDst {  // write the value of position i to (buf, rank, i + off)
+    int32_t rank;
+    uint8_t buf, pad[3];
+    int64_t off;
+};
+struct FusedMove {
+    int64_t n;
+    int32_t leaf_begin, nleaves;
+    int32_t dst_begin, ndst;
+};
+struct FusedSchedule {
+    std::vector<std::vector<FusedMove>> passes;
+    std::vector<FusedLeaf> leaves;
+    std::vector<FusedDst> dsts;
+    std::vector<int32_t> pass_levels;  // original levels per pass (0: the final copy of renamed results)
+    int64_t tmp_elems = 0;             // workspace elements per rank, renaming slots included
+};
+constexpr int kFuseMaxLeaves = 8;  // leaves of one fused value (2^3: three levels of sums)
+constexpr int kFuseMaxDsts = 8;    // destinations of one fused move
+constexpr int kFuseMaxDepth = 4;   // evaluation stack of one program
+
+// Fuses up to `depth` consecutive levels per pass (depth 1 keeps every
+// level but still drops writes nothing reads).  `out_rows[r]` tells whether
+// rank r's receive row is a result.  A pass whose values would need more
+// than kFuseMaxLeaves leaves or kFuseMaxDepth stack entries is split.  A
+// write that would overwrite an element another move of its pass still
+// reads goes to a fresh workspace slot (after the schedule's own workspace)
+// and later passes read it there; results left in slots are copied home by
+// a last pass.  The fused schedule is checked against the original by
+// symbolic execution (every result element the same addition tree); false
+// with `err` if not.
+bool fuse_schedule(const Schedule& s, int P, int depth, const std::vector<bool>& out_rows, FusedSchedule* out,
+                   std::string* err);
+
+// build_flow for a fused schedule: pieces index fused moves (pass order);
+// reads are every leaf, writes every destination.
+void build_flow_fused(const FusedSchedule& f, int P, int64_t piece_elems, int64_t min_item_elems,
+                      int64_t max_item_elems, int target_items, int max_pieces, FlowPlan* out);
+
 // Per-link byte counts of a message list on the torus: 2 * ndims directed
 // links per node, index (node * ndims + d) * 2 + (dir > 0 ? 0 : 1).
 // Routes are dimension-ordered and minimal per dimension (+ on ties).

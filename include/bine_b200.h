@@ -139,6 +139,19 @@ int bine_comm_set_engine(bine_comm_t comm, int engine);
  * message's first segment before its last one is ready); large ones cut
  * per-segment overhead.  Results do not depend on it. */
 int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes);
+
+/* Level fusion for the PIPELINED engine: `levels` consecutive levels of the
+ * reference's schedule per pass (1, the default: every level on its own, as
+ * the STEPS engine runs them).  Within a pass, values that one step hands to
+ * the next (partial sums, staged messages) stay in registers; a pass writes
+ * only what a later pass reads or what is a result, and a copy several ranks
+ * receive from one rank is read once.  A write that would overwrite what its
+ * pass still reads goes to a fresh workspace slot instead.  Results are
+ * bit-identical (the schedule's addition trees), and after every pass each
+ * element that is read later or is a result holds, at its own position or
+ * in its slot, what the reference's buffers hold after that step.  No
+ * counterpart in the reference. */
+int bine_comm_set_fusion(bine_comm_t comm, int levels);
 int bine_comm_set_float_order(bine_comm_t comm, int order);
 
 /* ----------------------------------------------------------- collectives */
@@ -379,13 +392,27 @@ int bine_plan_moves(bine_comm_t comm, bine_coll_t coll, long count, int root, in
  * first element, elements); items[n][5]: (first piece, end piece, first
  * dependency, end dependency, level); deps[n]: an item index, or -(l + 1)
  * for every item of level l.  `elem_size` and `target_items` stand for the
- * datatype and for the engine's four items per SM per level. */
+ * datatype and for the engine's four items per SM per level.  With level
+ * fusion set (bine_comm_set_fusion > 1) it is the fused plan: pieces index
+ * the moves of bine_plan_fused and levels are its passes. */
 int bine_plan_flow(bine_comm_t comm, bine_coll_t coll, long count, int root, int elem_size, int target_items,
                    int64_t *pieces, size_t piece_cap, size_t *n_pieces, int32_t *items, size_t item_cap,
                    size_t *n_items, int32_t *deps, size_t dep_cap, size_t *n_deps);
 
 int bine_plan_messages(bine_comm_t comm, bine_coll_t coll, long count, int root, int64_t *msgs, size_t cap,
                        size_t *n_msgs);
+
+/* The fused form of a call's schedule at `levels` levels per pass, as the
+ * PIPELINED engine runs it with bine_comm_set_fusion(levels), for tests and
+ * tools.  moves[n][6]: (pass, elements, first leaf, leaves, first
+ * destination, destinations); leaves[n][4]: (rank, buffer, additions after
+ * it, element offset of position 0) in postfix order; dsts[n][3]: (rank,
+ * buffer, element offset of position 0).  Counts and *tmp_elems (workspace
+ * elements per rank, renaming slots included) are always returned; arrays
+ * are filled when their capacity suffices. */
+int bine_plan_fused(bine_comm_t comm, bine_coll_t coll, long count, int root, int levels, int64_t *moves,
+                    size_t move_cap, size_t *n_moves, int64_t *leaves, size_t leaf_cap, size_t *n_leaves,
+                    int64_t *dsts, size_t dst_cap, size_t *n_dsts, int64_t *tmp_elems);
 
 /* Exact reduction trees (allreduce, reduce_scatter, reduce): postfix
  * programs of (rank, adds, shift) entries and output segments of

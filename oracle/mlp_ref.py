@@ -10,7 +10,10 @@ import math
 
 import numpy as np
 
-_erf = np.vectorize(math.erf)
+try:  # scipy's erf is a vectorised double-precision erf; math.erf otherwise
+    from scipy.special import erf as _erf
+except ImportError:  # pragma: no cover
+    _erf = np.vectorize(math.erf)
 
 
 def bf16(x):

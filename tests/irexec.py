@@ -57,3 +57,33 @@ def eval_trees(comm, coll, count, x, root=0):
         else:
             out[rank, off:off + n] = stack[0]
     return out
+
+
+def run_fused(comm, coll, count, x, root=0, levels=3):
+    """Executes the fused form of the schedule (bine_plan_fused) pass by
+    pass with value semantics; returns (receive rows, elements read and
+    written, passes)."""
+    P = comm.nranks
+    mv, lv, dv, tmp = comm.plan_fused(coll, count, root, levels)
+    se, re = bine.row_counts(coll, count, P)
+    bufs = [x.copy() if se else np.zeros((P, 0), x.dtype), np.zeros((P, re), x.dtype),
+            np.zeros((P, max(1, tmp)), x.dtype)]
+    if coll == "bcast":
+        bufs[1][root] = x[root]
+    traffic = 0
+    for p in np.unique(mv[:, 0]):
+        results = []
+        for _, n, lb, nl, db, nd in mv[mv[:, 0] == p]:
+            stack = []
+            for r, b, adds, off in lv[lb:lb + nl]:
+                stack.append(bufs[b][r, off:off + n].copy())
+                for _ in range(adds):
+                    top = stack.pop()
+                    stack[-1] = (stack[-1] + top).astype(x.dtype)
+            assert len(stack) == 1
+            traffic += n * (nl + nd)
+            for r, b, off in dv[db:db + nd]:
+                results.append((b, r, off, stack[0]))
+        for b, r, off, v in results:
+            bufs[b][r, off:off + len(v)] = v
+    return bufs[1], traffic, len(np.unique(mv[:, 0]))

@@ -52,16 +52,19 @@ def case_id(c):
             f"-r{c.get('root', 0)}-{c.get('family', 'BINE')}")
 
 
-@pytest.mark.parametrize("engine", ["fused", "steps", "pipelined", "pipelined-seg256"])
+@pytest.mark.parametrize("engine", ["fused", "steps", "pipelined", "pipelined-seg256", "pipelined-fuse3",
+                                    "pipelined-fuse6-seg256", "pipelined-fuse64"])
 @pytest.mark.parametrize("case", CASES, ids=case_id)
 def test_engine_matches_reference(case, engine):
     x = case_input(case)
     root = case.get("root", 0)
     segment = 256 if engine.endswith("seg256") else 0  # many small segments, level dependencies
+    fusion = int(engine.split("fuse")[1].split("-")[0]) if "fuse" in engine else 1  # levels per pass
     engine = engine.split("-")[0]
     comm = make_comm(case["P"], case["coll"], case["variant"], case.get("dims"), case.get("ports", 1),
                      case.get("family", "BINE"), case.get("distance"), engine)
     comm.set_segment(segment)
+    comm.set_fusion(fusion)
     rr = receiving_ranks(case["coll"], case["P"], root)
     reduction = case["coll"] in ("allreduce", "reduce_scatter", "reduce")
     right = reference_is_right(case, x)
@@ -599,3 +602,49 @@ def test_ring_allreduce_matches_the_oracle(engine, dims, count):
         got = run(comm, "allreduce", x, count)
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), dt
     comm.close()
+
+
+@pytest.mark.parametrize("levels", [3, 6, 10])
+@pytest.mark.parametrize("coll,variant,P,count", [
+    ("allreduce", "B", 256, 256 * 64 + 7), ("allreduce", "B", 96, 96 * 40), ("allreduce", "L", 64, 4096),
+    ("reduce_scatter", "VEC_HALVING_CONT_PERMUTE", 128, 300), ("allgather", "VEC_DOUBLING_CONT_PERMUTE", 128, 301),
+    ("alltoall", "LOG", 128, 33), ("bcast", "BINOMIAL_TREE", 128, 5000), ("reduce", "BINOMIAL_TREE", 64, 999)])
+def test_fused_pipelined_engine_matches_the_level_by_level_engine(coll, variant, P, count, levels):
+    """Level fusion on larger schedules: the PIPELINED engine with fused
+    passes gives the STEPS engine's bytes (float32 in the reference order
+    included), on two calls in a row and in place."""
+    rr = receiving_ranks(coll, P, 0)
+    for dt in (np.int32, np.float32):
+        sc, _ = buffer_counts(coll, count, P)
+        rng = np.random.default_rng(P + count + levels)
+        x = (rng.integers(-1000, 1001, (P, sc)) if dt == np.int32 else rng.standard_normal((P, sc))).astype(dt)
+        want = run(make_comm(P, coll, variant, engine="steps"), coll, x, count)
+        comm = make_comm(P, coll, variant, engine="pipelined")
+        comm.set_fusion(levels)
+        for _ in range(2):
+            got = run(comm, coll, x, count)
+            assert np.array_equal(got[rr].view(np.uint8), want[rr].view(np.uint8)), (dt, levels)
+        if coll == "allreduce":
+            buf = torch.from_numpy(x).cuda()
+            comm.allreduce(buf, buf, count, NP2CODE[x.dtype])
+            comm.synchronize()
+            assert np.array_equal(buf.cpu().numpy().view(np.uint8), want.view(np.uint8))
+
+
+def test_fused_pipelined_engine_timeout_is_reported_and_recoverable():
+    """The fused kernel's segment waits are bounded like the unfused ones."""
+    P, count = 16, 16 * 64
+    x = np.random.default_rng(6).integers(-1000, 1001, (P, count)).astype(np.int32)
+    comm = make_comm(P, "allreduce", "B", engine="pipelined")
+    comm.set_fusion(3)
+    comm.set_step_timeout(200)
+    comm.debug_set_barrier_extra(1)
+    send = torch.from_numpy(x).cuda()
+    recv = torch.zeros_like(send)
+    comm.allreduce(send, recv, count, bine.INT32)
+    with pytest.raises(bine.Timeout):
+        comm.synchronize()
+    comm.debug_set_barrier_extra(0)
+    comm.allreduce(send, recv, count, bine.INT32)
+    comm.synchronize()
+    assert np.array_equal(recv.cpu().numpy(), expected("allreduce", x, P, count))
