@@ -49,7 +49,9 @@ def configure(args):
     ALGO_BYTES = 2 * P_RANKS * COUNT * ES
     if (args.P, args.count, args.dtype, args.engine) != (256, 1 << 20, "int32", "fused"):
         WORKLOAD = (f"Bine allreduce (variant B, 1 port, 1-D ring), P={P_RANKS} virtual ranks, {COUNT} {args.dtype} "
-                    f"per rank, MPI_SUM, {args.engine} engine, {args.order} float order"
+                    f"per rank, MPI_SUM, {args.engine} engine"
+                    + (f" ({args.fusion} levels per pass)" if args.engine == "pipelined" and args.fusion > 1 else "")
+                    + f", {args.order} float order"
                     + (f", {args.tree_split} lanes per vector" if args.tree_split else "") + " (profiling variant)")
 METRIC = "virtual-rank Bine allreduce GB/s"
 WORKLOAD = "Bine allreduce (variant B, 1 port, 1-D ring), P=256 virtual ranks, 1,048,576 int32 (4 MiB) per rank, MPI_SUM"
@@ -233,6 +235,7 @@ def run_engine_arm(args):
     comm.set_stream(stream)
     comm.set_algo("allreduce", "B")
     comm.set_engine(args.engine)
+    comm.set_fusion(args.fusion)
     comm.set_float_order(args.order)
     comm.set_tree_split(args.tree_split)
     comm.set_host_window(args.host_window)
@@ -838,15 +841,19 @@ def run_sweep_suite(args):
             f.write(json.dumps(r) + "\n")
             f.flush()
 
-        for P in SWEEP_P:
+        sweep_p = [int(v) for v in args.sweep_p.split(",")] if args.sweep_p else SWEEP_P
+        for P in sweep_p:
             comms = {}
-            for engine in SWEEP_ENGINES:
+            engines = SWEEP_ENGINES + ((f"pipelined-fuse{args.sweep_fusion}",) if args.sweep_fusion > 1 else ())
+            for engine in engines:
                 cm = bine.Comm(P)
-                cm.set_engine(engine)
+                cm.set_engine(engine.split("-")[0])
+                if "-fuse" in engine:
+                    cm.set_fusion(args.sweep_fusion)
                 cm.set_stream(stream)
                 comms[engine] = cm
             for coll in SWEEP_COLLS:
-                for nbytes in SWEEP_BYTES:
+                for nbytes in [b for b in SWEEP_BYTES if b >= args.sweep_min_bytes]:
                     for dname, tdt, code, es in dtypes:
                         count = max(1, nbytes // es)
                         se, re = bine.row_counts(coll, count, P)
@@ -865,7 +872,7 @@ def run_sweep_suite(args):
                         recv = torch.zeros((P, re), dtype=tdt, device="cuda")
                         if coll == "bcast":
                             recv[0] = send[0]
-                        for engine in SWEEP_ENGINES:
+                        for engine in engines:
                             if engine != "fused" and P > 384:
                                 continue
                             comm = comms[engine]
@@ -943,7 +950,18 @@ def run_sweep_suite(args):
             band = "below 64 KiB" if nb < 65536 else ("64 KiB to 2 MiB" if nb < 2 << 20 else "2 MiB and up")
             ratio.setdefault(band, []).append(t / us[(coll, P, nb, dt, "pipelined")])
     sums = [r for r in timed if r["dtype"] == "float32" and r["coll"] in ("allreduce", "reduce_scatter")]
+    big = {}
+    for r in timed:
+        if r["bytes_per_rank"] >= 2 << 20:
+            big.setdefault((r["coll"], r["engine"]), []).append(r["algo_gbs"])
+    fuse_ratio = {}
+    for (coll, P, nb, dt, eng), t in us.items():
+        if eng.startswith("pipelined-fuse") and (coll, P, nb, dt, "pipelined") in us:
+            band = "below 64 KiB" if nb < 65536 else ("64 KiB to 2 MiB" if nb < 2 << 20 else "2 MiB and up")
+            fuse_ratio.setdefault(band, []).append(us[(coll, P, nb, dt, "pipelined")] / t)
     line = {"suite": "sweep", "points_timed": len(timed), "points_incorrect": len(bad),
+            "pipelined_over_fused_passes_time_geomean": {k: round(float(np.exp(np.mean(np.log(v)))), 3)
+                                                         for k, v in sorted(fuse_ratio.items())},
             "float_sums_bit_exact_vs_oracle": len([r for r in sums if r["float_order"] == "reference" and r["correct"]]),
             "float_sums_fast_within_1e-6_of_fp64": len([r for r in sums if r["float_order"] == "fast" and r["correct"]]),
             "timing": "median of per-call CUDA-event times, L2 flushed (256 MiB written) before every call",
@@ -955,6 +973,7 @@ def run_sweep_suite(args):
             if any("speedup" in r for r in refs) else None,
             "points_unsupported": len([r for r in rows if "unsupported" in r]), "points_skipped": len(skipped),
             "best_algo_gbs": {f"{k[0]}/{k[1]}": round(v["algo_gbs"], 1) for k, v in sorted(best.items())},
+            "median_algo_gbs_2mib_up": {f"{c}/{e}": round(float(np.median(v)), 1) for (c, e), v in sorted(big.items())},
             "seconds": round(time.time() - t_start, 1), "jsonl": os.path.relpath(path, ROOT)}
     print(json.dumps(line))
     return 0 if not bad else 1
@@ -1235,6 +1254,12 @@ def main():
     ap.add_argument("--count", type=int, default=1 << 20)
     ap.add_argument("--dtype", default="int32", choices=["int32", "float"])
     ap.add_argument("--engine", default="fused", choices=["fused", "steps", "pipelined"])
+    ap.add_argument("--fusion", type=int, default=1,
+                    help="levels of the schedule per pass of the pipelined engine (profiling variant)")
+    ap.add_argument("--sweep-fusion", type=int, default=0,
+                    help="also time the pipelined engine with this many levels per pass in the sweep")
+    ap.add_argument("--sweep-p", default=None, help="comma-separated P values of the sweep (default: all)")
+    ap.add_argument("--sweep-min-bytes", type=int, default=0, help="smallest per-rank message of the sweep")
     ap.add_argument("--order", default="reference", choices=["reference", "fast"])
     ap.add_argument("--host-window", type=int, default=32 << 20,
                     help="column-window bytes of the host-buffer pipeline (e2e leg)")
