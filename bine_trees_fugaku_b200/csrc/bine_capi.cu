@@ -128,6 +128,9 @@ struct DevTrees {
     int natiles = 0;
     int max_prog_len = 0;
     int depth = 0;  // deepest evaluation stack of any program
+    // Some rank has its own trees (other ranks' tiles write rows that its
+    // tiles read at the same columns).
+    bool per_rank = false;
     // Split form (k_tree_split), used when split_k > 1 and the layout is
     // 16-byte aligned: the same segments over the split programs.
     int split_k = 1;
@@ -533,8 +536,14 @@ int fused_schedule(bine_comm_t c, const PlanKey& k, int levels, std::shared_ptr<
     return BINE_SUCCESS;
 }
 
+// Levels per pass of the automatic fusion setting, per collective.
+constexpr int kAutoFusion[kNumColls] = {3, 4, 6, 4, 3, 10, 6, 6};
+
+int fusion_levels(bine_comm_t c, int coll) { return c->fusion > 0 ? c->fusion : kAutoFusion[coll]; }
+
 int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFused>* out) {
-    const FusedKey key{PlanKeyEs{k, es, c->segment_bytes}, c->fusion};
+    const int levels = fusion_levels(c, k.coll);
+    const FusedKey key{PlanKeyEs{k, es, c->segment_bytes}, levels};
     {
         std::lock_guard<std::mutex> lk(c->mu);
         auto it = c->dev_fused.find(key);
@@ -545,7 +554,7 @@ int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFu
     }
     std::shared_ptr<Schedule> s;
     FusedSchedule fs;
-    int rc = fused_schedule(c, k, c->fusion, &s, &fs);
+    int rc = fused_schedule(c, k, levels, &s, &fs);
     if (rc) return rc;
     // Every row range the kernel will touch must lie inside its row.
     const int64_t rows[3] = {s->send_elems, s->recv_elems, fs.tmp_elems};
@@ -647,6 +656,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
     for (const OutSegment& sg : tp.segs) {
         segs.push_back(dev::TreeSeg{sg.off, sg.n, sg.rank, sg.prog_begin, sg.prog_len, sg.depth});
         d->max_prog_len = std::max(d->max_prog_len, sg.prog_len);
+        d->per_rank |= sg.rank >= 0 && k.coll == kAllreduce;
     }
     // Every segment whose program reads at 16-byte-aligned shifts gets a
     // vector body: its elements from the first to the last 16-byte boundary
@@ -1299,11 +1309,23 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
     // kernels and the reduce_scatter tiles write rows that other blocks still
     // read.  Such calls take their input rows from a staged copy.  The one
     // exception is an allreduce or reduce on the FUSED engine whose arrays
-    // are one (same base, same stride): every tile reads its columns of all
-    // rows before writing the same columns, and no other tile touches them.
-    if (arrays_overlap(in, ist, (size_t)se * es, out, ost, (size_t)re * es, c->P) &&
-        !(c->engine == BINE_ENGINE_FUSED && (coll == kAllreduce || coll == kReduce) &&
-          (const void*)in == (const void*)out && ist == ost)) {
+    // are one (same base, same stride) and whose columns each have one
+    // writing tile: that tile reads its columns of all rows before writing
+    // them, and no other tile touches them.  Per-rank float trees (the L
+    // butterfly in the reference order) give one tile per rank and column,
+    // so they are staged too.
+    bool alias_safe = c->engine == BINE_ENGINE_FUSED && (coll == kAllreduce || coll == kReduce) &&
+                      (const void*)in == (const void*)out && ist == ost;
+    if (alias_safe && coll == kAllreduce && (dt == BINE_FLOAT || dt == BINE_DOUBLE) &&
+        c->order == BINE_ORDER_REFERENCE) {
+        // Per-rank addition trees (the L butterfly): the tile of one rank's
+        // row reads, at the same columns, the rows other tiles write.
+        std::shared_ptr<DevTrees> d;
+        rc = get_dev_trees(c, k, es, &d);
+        if (rc) return rc;
+        alias_safe = !d->per_rank;
+    }
+    if (arrays_overlap(in, ist, (size_t)se * es, out, ost, (size_t)re * es, c->P) && !alias_safe) {
         const size_t pitch = ((size_t)se * es + 255) / 256 * 256, bytes = pitch * (size_t)c->P;
         if (c->inplace_bytes < bytes) {
             CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1324,7 +1346,7 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
         if (rc) return rc;
         return launch_steps_dt(c, dt, *d, in, ist, out, ost);
     }
-    if (c->engine == BINE_ENGINE_PIPELINED && c->fusion > 1) {
+    if (c->engine == BINE_ENGINE_PIPELINED && fusion_levels(c, coll) > 1) {
         std::shared_ptr<DevFused> d;
         rc = get_dev_fused(c, k, es, &d);
         if (rc) return rc;
@@ -1989,7 +2011,7 @@ int bine_comm_set_algo(bine_comm_t comm, bine_coll_t coll, int variant, int fami
 
 int bine_comm_set_fusion(bine_comm_t comm, int levels) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
-    if (levels < 1 || levels > 64) return fail(BINE_ERR_ARG, "levels per pass must be in [1, 64]");
+    if (levels < 0 || levels > 64) return fail(BINE_ERR_ARG, "levels per pass must be in [0, 64]");
     comm->fusion = levels;
     return BINE_SUCCESS;
 }
@@ -2184,10 +2206,10 @@ int bine_plan_flow(bine_comm_t comm, bine_coll_t coll, long count, int root, int
     int rc = plan_for_query(comm, coll, count, root, &s);
     if (rc) return rc;
     FlowPlan fp;
-    if (comm->fusion > 1) {
+    if (fusion_levels(comm, coll) > 1) {
         // The fused plan: pieces index the fused moves in pass order.
         FusedSchedule fs;
-        rc = fused_schedule(comm, make_key(comm, coll, count, root), comm->fusion, &s, &fs);
+        rc = fused_schedule(comm, make_key(comm, coll, count, root), fusion_levels(comm, coll), &s, &fs);
         if (rc) return rc;
         const int64_t piece = comm->segment_bytes > 0 ? std::max<int64_t>(16, comm->segment_bytes / elem_size) : 0;
         build_flow_fused(fs, comm->P, piece, std::max<int64_t>(1, 4096 / elem_size), kFlowMaxItemBytes / elem_size,

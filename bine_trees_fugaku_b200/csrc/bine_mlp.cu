@@ -182,7 +182,7 @@ unsigned grid1(long long n) { return (unsigned)std::max(1LL, std::min((n + 255) 
 constexpr int kEnsMaxModels = 8;  // portable cluster size
 constexpr int kEnsH = 256;        // hidden width the fused kernel is built for
 constexpr int kEnsMaxOut = 256;
-constexpr int kEnsThreads = 256;
+constexpr int kEnsThreads = 1024;  // 32 warps: one 8-column tile each (widths up to 256)
 
 struct EnsModel {
     const bf16* wb;   // bf16 weights (layer l at woff[l], [out][in] row-major)
@@ -206,56 +206,50 @@ __device__ __forceinline__ void mma_bf16_16816(float* d, const uint32_t* a, cons
 
 // One layer for 16 rows: out[16][N] = act[16][K] W^T + bias, then GELU into
 // the next activation buffer (hidden) or fp32 into `outf` (last layer).
-// Warp w computes the n-tiles w, w + 8, ... (8 columns each), up to kNT per
-// pass, sharing each A fragment across them.
-template <int kNT>
+// Warp w owns the n-tile w (8 columns; N <= 8 * warps).  It first loads all
+// of that tile's weight fragments for the whole K (at most 16 k-steps, two
+// 32-bit registers each), so the layer costs one round of L2 latency rather
+// than one per k-step, then runs its mma chain from the activations in
+// shared memory.
 __device__ __forceinline__ void ens_layer(const bf16* __restrict__ act, int lda, int K, const bf16* __restrict__ W,
-                                          const float* __restrict__ bias, int N, bf16* next, int ldn,
-                                          float* outf, int ldo) {
+                                          const float* __restrict__ bias, int N, bf16* next, int ldn, float* outf,
+                                          int ldo) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int ntiles = N / 8;
-    for (int j0 = warp; j0 < ntiles; j0 += 8 * kNT) {
-        float acc[kNT][4];
+    const int j = warp;
+    if (j * 8 >= N) return;
+    const int ksteps = K / 16;
+    uint32_t b[16][2];
+    const bf16* wr = W + (size_t)(j * 8 + g) * K + 2 * t;
 #pragma unroll
-        for (int q = 0; q < kNT; q++)
+    for (int kk = 0; kk < 16; kk++)
+        if (kk < ksteps) {
+            b[kk][0] = __ldg((const unsigned int*)(wr + kk * 16));
+            b[kk][1] = __ldg((const unsigned int*)(wr + kk * 16 + 8));
+        }
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int e = 0; e < 4; e++) acc[q][e] = 0.f;
-        for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int kk = 0; kk < 16; kk++)
+        if (kk < ksteps) {
+            const int k0 = kk * 16;
             uint32_t a[4];
             a[0] = *(const uint32_t*)(act + g * lda + k0 + 2 * t);
             a[1] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 2 * t);
             a[2] = *(const uint32_t*)(act + g * lda + k0 + 8 + 2 * t);
             a[3] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 8 + 2 * t);
-#pragma unroll
-            for (int q = 0; q < kNT; q++) {
-                const int j = j0 + q * 8;
-                if (j < ntiles) {
-                    const bf16* wr = W + (size_t)(j * 8 + g) * K + k0 + 2 * t;
-                    uint32_t b[2];
-                    b[0] = __ldg((const unsigned int*)wr);
-                    b[1] = __ldg((const unsigned int*)(wr + 8));
-                    mma_bf16_16816(acc[q], a, b);
-                }
-            }
+            mma_bf16_16816(acc, a, b[kk]);
         }
-#pragma unroll
-        for (int q = 0; q < kNT; q++) {
-            const int j = j0 + q * 8;
-            if (j >= ntiles) continue;
-            const int c = j * 8 + 2 * t;
-            const float b0 = bias[c], b1 = bias[c + 1];
-            const float v[4] = {acc[q][0] + b0, acc[q][1] + b1, acc[q][2] + b0, acc[q][3] + b1};
-            if (next) {
-                *(__nv_bfloat162*)(next + g * ldn + c) = __floats2bfloat162_rn(gelu(v[0]), gelu(v[1]));
-                *(__nv_bfloat162*)(next + (g + 8) * ldn + c) = __floats2bfloat162_rn(gelu(v[2]), gelu(v[3]));
-            } else {
-                outf[g * ldo + c] = v[0];
-                outf[g * ldo + c + 1] = v[1];
-                outf[(g + 8) * ldo + c] = v[2];
-                outf[(g + 8) * ldo + c + 1] = v[3];
-            }
-        }
+    const int c = j * 8 + 2 * t;
+    const float b0 = bias[c], b1 = bias[c + 1];
+    const float v[4] = {acc[0] + b0, acc[1] + b1, acc[2] + b0, acc[3] + b1};
+    if (next) {
+        *(__nv_bfloat162*)(next + g * ldn + c) = __floats2bfloat162_rn(gelu(v[0]), gelu(v[1]));
+        *(__nv_bfloat162*)(next + (g + 8) * ldn + c) = __floats2bfloat162_rn(gelu(v[2]), gelu(v[3]));
+    } else {
+        outf[g * ldo + c] = v[0];
+        outf[g * ldo + c + 1] = v[1];
+        outf[(g + 8) * ldo + c] = v[2];
+        outf[(g + 8) * ldo + c + 1] = v[3];
     }
 }
 
@@ -277,7 +271,7 @@ __global__ void __launch_bounds__(kEnsThreads) k_mlp_ensemble(EnsArgs a) {
     for (int l = 0; l < 4; l++) {
         const bf16* in = s_act[l & 1];
         bf16* nxt = l < 3 ? s_act[(l + 1) & 1] : nullptr;
-        ens_layer<4>(in, kLd, dims[l], M.wb + a.woff[l], M.w + a.boff[l], dims[l + 1], nxt, kLd, s_out, a.dout);
+        ens_layer(in, kLd, dims[l], M.wb + a.woff[l], M.w + a.boff[l], dims[l + 1], nxt, kLd, s_out, a.dout);
         __syncthreads();
     }
     cluster.sync();

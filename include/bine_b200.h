@@ -9,7 +9,8 @@
  * with MPI_IN_PLACE, or rows that interleave): such a call first copies its
  * input rows to a staging area of the communicator, except an allreduce or
  * reduce on the FUSED engine whose two arrays are identical (same base and
- * stride), which needs no copy.  Calls are asynchronous and ordered on the
+ * stride) and whose result is one value per column (not per-rank float
+ * trees), which needs no copy.  Calls are asynchronous and ordered on the
  * communicator's CUDA stream.  Functions return BINE_SUCCESS or an error code and never abort;
  * bine_last_error_string() describes the last error of the calling thread.
  *
@@ -150,7 +151,9 @@ int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes);
  * bit-identical (the schedule's addition trees), and after every pass each
  * element that is read later or is a result holds, at its own position or
  * in its slot, what the reference's buffers hold after that step.  No
- * counterpart in the reference. */
+ * counterpart in the reference.  0 chooses the levels per pass for each
+ * collective (allreduce and reduce 3, reduce_scatter and bcast 4, allgather,
+ * scatter and gather 6, alltoall 10). */
 int bine_comm_set_fusion(bine_comm_t comm, int levels);
 int bine_comm_set_float_order(bine_comm_t comm, int order);
 

@@ -227,3 +227,23 @@ def test_fused_dataflow_plan_orders_every_conflict_and_matches_reference(case):
         out = run_items(case, x, mv, lv, dv, tmp, pieces, items, deps, seed=levels + segment)
         rr = receiving_ranks(case["coll"], case["P"], root)
         assert np.array_equal(out[rr].view(np.uint8), case["out"][rr].view(np.uint8))
+
+
+def test_automatic_fusion_uses_the_per_collective_levels():
+    """bine_comm_set_fusion(0): each collective takes its own levels per pass
+    (allreduce and reduce 3, reduce_scatter and bcast 4, allgather, scatter
+    and gather 6, alltoall 10); the dataflow plan is that fused plan."""
+    table = {"allreduce": ("B", 3), "reduce_scatter": ("VEC_HALVING_CONT_PERMUTE", 4),
+             "allgather": ("VEC_DOUBLING_CONT_PERMUTE", 6), "bcast": ("BINOMIAL_TREE", 4),
+             "reduce": ("BINOMIAL_TREE", 3), "alltoall": ("LOG", 10)}
+    for coll, (variant, levels) in table.items():
+        count = 16 * 9 + 1 if coll in ("allreduce", "bcast", "reduce") else 5
+        auto = bine.Comm(16)
+        auto.set_algo(coll, variant)
+        auto.set_fusion(0)
+        fixed = bine.Comm(16)
+        fixed.set_algo(coll, variant)
+        fixed.set_fusion(levels)
+        a = auto.plan_flow(coll, count, 0, 4, 592)
+        b = fixed.plan_flow(coll, count, 0, 4, 592)
+        assert all(np.array_equal(x, y) for x, y in zip(a, b)), coll
