@@ -50,7 +50,7 @@ def configure(args):
     if (args.P, args.count, args.dtype, args.engine) != (256, 1 << 20, "int32", "fused"):
         WORKLOAD = (f"Bine allreduce (variant B, 1 port, 1-D ring), P={P_RANKS} virtual ranks, {COUNT} {args.dtype} "
                     f"per rank, MPI_SUM, {args.engine} engine"
-                    + (f" ({args.fusion} levels per pass)" if args.engine == "pipelined" and args.fusion > 1 else "")
+                    + (f" ({args.fusion or 'automatic'} levels per pass)" if args.engine == "pipelined" else "")
                     + f", {args.order} float order"
                     + (f", {args.tree_split} lanes per vector" if args.tree_split else "") + " (profiling variant)")
 METRIC = "virtual-rank Bine allreduce GB/s"
@@ -235,7 +235,8 @@ def run_engine_arm(args):
     comm.set_stream(stream)
     comm.set_algo("allreduce", "B")
     comm.set_engine(args.engine)
-    comm.set_fusion(args.fusion)
+    if args.fusion is not None:
+        comm.set_fusion(args.fusion)
     comm.set_float_order(args.order)
     comm.set_tree_split(args.tree_split)
     comm.set_host_window(args.host_window)
@@ -844,7 +845,7 @@ def run_sweep_suite(args):
         sweep_p = [int(v) for v in args.sweep_p.split(",")] if args.sweep_p else SWEEP_P
         for P in sweep_p:
             comms = {}
-            engines = SWEEP_ENGINES + ((f"pipelined-fuse{args.sweep_fusion}",) if args.sweep_fusion > 1 else ())
+            engines = SWEEP_ENGINES + ((f"pipelined-fuse{args.sweep_fusion}",) if args.sweep_fusion >= 1 else ())
             for engine in engines:
                 cm = bine.Comm(P)
                 cm.set_engine(engine.split("-")[0])
@@ -1204,6 +1205,31 @@ def run_picker_suite(args):
         ens.forward(x16, out=y16)
     e1.record()
     torch.cuda.synchronize()
+    # Device time of one fused forward: 20 forwards captured in a CUDA
+    # graph (no host launch cost between them), replayed.
+    forward16_device_us = None
+    try:
+        gs = torch.cuda.Stream()
+        gs.wait_stream(torch.cuda.current_stream())
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(gs):
+            with torch.cuda.graph(gr, stream=gs):
+                for _ in range(20):
+                    ens.forward(x16, stream=gs, out=y16)
+        torch.cuda.current_stream().wait_stream(gs)
+        for _ in range(3):
+            gr.replay()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(10):
+            gr.replay()
+        g1.record()
+        torch.cuda.synchronize()
+        forward16_device_us = g0.elapsed_time(g1) * 1e3 / 200
+        del gr
+    except RuntimeError as e:
+        print(f"graph timing of the ensemble forward failed: {e}", file=sys.stderr)
     # The layered path (per model: one GEMM + bias/GELU launch per layer),
     # for comparison.
     for _ in range(3):
@@ -1230,9 +1256,12 @@ def run_picker_suite(args):
             "train_loss_first_last": [losses[0], float(np.mean(losses[-50:]))],
             "measure_s": t_measure, "train_s": t_train,
             "forward16_us": e0.elapsed_time(e1) * 10.0,
+            "forward16_device_us": forward16_device_us,
             "forward16_layered_us": l0.elapsed_time(l1) * 10.0,
             "forward16_note": "ensemble mean of a 16-row batch: one fused launch (bine_mlp_ensemble_forward) "
-                              "against the layered per-model path",
+                              "against the layered per-model path; forward16_us includes the host's launch "
+                              "cost (back-to-back calls from Python), forward16_device_us is device time "
+                              "(20 forwards per CUDA graph replay)",
             "config": {"model": "ensemble of bine_mlp 16-256-256-256-%d GELU, bf16 weights, fp32 accumulate" % pk.OUT_DIM,
                        "engine": "steps", "timing": "per arm: median of 3 CUDA-event batches of back-to-back "
                                                     "launches (each batch ~300 us, at most 32 launches)",
@@ -1258,10 +1287,10 @@ def main():
     ap.add_argument("--count", type=int, default=1 << 20)
     ap.add_argument("--dtype", default="int32", choices=["int32", "float"])
     ap.add_argument("--engine", default="fused", choices=["fused", "steps", "pipelined"])
-    ap.add_argument("--fusion", type=int, default=1,
-                    help="levels of the schedule per pass of the pipelined engine (profiling variant)")
+    ap.add_argument("--fusion", type=int, default=None,
+                    help="levels of the schedule per pass of the pipelined engine (default: the engine's own choice)")
     ap.add_argument("--sweep-fusion", type=int, default=0,
-                    help="also time the pipelined engine with this many levels per pass in the sweep")
+                    help="also time the pipelined engine with this many levels per pass (1: level by level)")
     ap.add_argument("--sweep-p", default=None, help="comma-separated P values of the sweep (default: all)")
     ap.add_argument("--sweep-min-bytes", type=int, default=0, help="smallest per-rank message of the sweep")
     ap.add_argument("--order", default="reference", choices=["reference", "fast"])

@@ -224,7 +224,7 @@ class Comm:
         self.ports = 1
         self.engine = "fused"
         self.float_order = "reference"
-        self.fusion = 1
+        self.fusion = 0
 
     def close(self):
         if getattr(self, "_h", None):
@@ -266,7 +266,7 @@ class Comm:
 
     def set_fusion(self, levels):
         """Levels of the reference's schedule per pass of the PIPELINED
-        engine (1: every level on its own)."""
+        engine (1: every level on its own; 0, the default: per collective)."""
         check(lib().bine_comm_set_fusion(self._h, levels))
         self.fusion = levels
 

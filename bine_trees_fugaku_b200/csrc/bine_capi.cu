@@ -233,7 +233,7 @@ struct bine_comm_s {
     std::unordered_map<PlanKeyEs, std::shared_ptr<DevSteps>, PlanKeyEsHash> dev_steps;
     std::unordered_map<PlanKeyEs, std::shared_ptr<DevTrees>, PlanKeyEsHash> dev_trees;
     std::unordered_map<FusedKey, std::shared_ptr<DevFused>, FusedKeyHash> dev_fused;
-    int fusion = 1;  // levels per pass of the PIPELINED engine (1: every level on its own)
+    int fusion = 0;  // levels per pass of the PIPELINED engine (0: per collective, 1: every level on its own)
     std::unordered_map<StructKey, int, StructKeyHash> verified;  // 1: proven, 0: refuted
     std::unordered_map<StructKey, std::string, StructKeyHash> refuted_why;
     long long segment_bytes = 0;
@@ -536,13 +536,34 @@ int fused_schedule(bine_comm_t c, const PlanKey& k, int levels, std::shared_ptr<
     return BINE_SUCCESS;
 }
 
-// Levels per pass of the automatic fusion setting, per collective.
-constexpr int kAutoFusion[kNumColls] = {3, 4, 6, 4, 3, 10, 6, 6};
+// Levels per pass of the automatic fusion setting, per collective
+// (allreduce, reduce_scatter, allgather, bcast, reduce, alltoall, scatter,
+// gather).  Measured on B200 at P = 64 and 256 from 512 KiB per rank: the
+// reductions run fastest at 6 (allreduce B 2.32 TB/s against 2.05 at 10),
+// the copies at 10 and more (allgather 5.07 TB/s against 1.99 at 6);
+// alltoall has about three IR levels per Bine step, and 13 keeps two passes.
+constexpr int kAutoFusion[kNumColls] = {6, 6, 12, 12, 6, 13, 12, 12};
 
-int fusion_levels(bine_comm_t c, int coll) { return c->fusion > 0 ? c->fusion : kAutoFusion[coll]; }
+// Planning a fused schedule costs about 4 us per move on the host (11 s for
+// allreduce B and 47 s for alltoall at P = 1024, once per call shape), so
+// the automatic setting runs larger schedules level by level.
+constexpr int64_t kAutoFusionMaxMoves = 1 << 20;
+
+int fusion_levels(bine_comm_t c, int coll, const Schedule* s = nullptr) {
+    if (c->fusion > 0) return c->fusion;
+    if (s) {
+        int64_t moves = 0;
+        for (const auto& lvl : s->levels) moves += (int64_t)lvl.size();
+        if (moves > kAutoFusionMaxMoves) return 1;
+    }
+    return kAutoFusion[coll];
+}
 
 int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFused>* out) {
-    const int levels = fusion_levels(c, k.coll);
+    std::shared_ptr<Schedule> sch;
+    int rc0 = get_schedule(c, k, &sch);
+    if (rc0) return rc0;
+    const int levels = fusion_levels(c, k.coll, sch.get());
     const FusedKey key{PlanKeyEs{k, es, c->segment_bytes}, levels};
     {
         std::lock_guard<std::mutex> lk(c->mu);
@@ -1346,7 +1367,12 @@ int run_collective(bine_comm_t c, int coll, const void* sendbuf, void* recvbuf, 
         if (rc) return rc;
         return launch_steps_dt(c, dt, *d, in, ist, out, ost);
     }
-    if (c->engine == BINE_ENGINE_PIPELINED && fusion_levels(c, coll) > 1) {
+    std::shared_ptr<Schedule> sched;
+    if (c->engine == BINE_ENGINE_PIPELINED) {
+        rc = get_schedule(c, k, &sched);
+        if (rc) return rc;
+    }
+    if (c->engine == BINE_ENGINE_PIPELINED && fusion_levels(c, coll, sched.get()) > 1) {
         std::shared_ptr<DevFused> d;
         rc = get_dev_fused(c, k, es, &d);
         if (rc) return rc;
@@ -2206,10 +2232,10 @@ int bine_plan_flow(bine_comm_t comm, bine_coll_t coll, long count, int root, int
     int rc = plan_for_query(comm, coll, count, root, &s);
     if (rc) return rc;
     FlowPlan fp;
-    if (fusion_levels(comm, coll) > 1) {
+    if (fusion_levels(comm, coll, s.get()) > 1) {
         // The fused plan: pieces index the fused moves in pass order.
         FusedSchedule fs;
-        rc = fused_schedule(comm, make_key(comm, coll, count, root), fusion_levels(comm, coll), &s, &fs);
+        rc = fused_schedule(comm, make_key(comm, coll, count, root), fusion_levels(comm, coll, s.get()), &s, &fs);
         if (rc) return rc;
         const int64_t piece = comm->segment_bytes > 0 ? std::max<int64_t>(16, comm->segment_bytes / elem_size) : 0;
         build_flow_fused(fs, comm->P, piece, std::max<int64_t>(1, 4096 / elem_size), kFlowMaxItemBytes / elem_size,

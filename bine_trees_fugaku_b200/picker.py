@@ -50,13 +50,19 @@ for v in ["VEC_DOUBLING_CONT_PERMUTE", "VEC_DOUBLING_CONT_SEND", "VEC_DOUBLING_B
     for p in PORTS:
         for s in SEGMENTS:
             ARMS.append(("allgather", v, p, s))
+# The reference's RING family (the bucket allreduce, its comparator): one
+# schedule whatever the port setting.
+for s in SEGMENTS:
+    ARMS.append(("allreduce", "RING", 1, s))
 NARMS = len(ARMS)
 IN_DIM = 16
 OUT_DIM = ((2 * NARMS + 15) // 16) * 16
 OPS = ["allreduce", "reduce_scatter", "allgather"]
-# Planning the per-block B schedules costs O(P^2 * ports) on the host; arms
-# beyond these sizes are not offered.
-MAX_P = {"B": 128, "B_COALESCE": 256}
+# Planning the per-block B schedules costs O(P^2 * ports) on the host, and
+# the bucket ring sends P messages per step for every step of every ring
+# (67 M moves at P = 4096 on one ring); arms beyond these sizes are not
+# offered.
+MAX_P = {"B": 128, "B_COALESCE": 256, "RING": 256}
 
 
 def is_p2(x):
@@ -105,6 +111,8 @@ def statically_valid(arm, coll, P, count, dims=None):
             return False
         if v == "B_CONT" and not is_p2(P):
             return False
+        if v == "RING":
+            return count >= 1
         if v != "L" and count < ports * P:
             return False
         if v == "L" and count < ports:
@@ -174,7 +182,10 @@ def order_bound(coll, datatype, engine="steps", float_order="reference"):
 
 
 def keep_of(comm, coll):
-    """The caller's (variant, ports) for `coll` on `comm`."""
+    """The caller's (variant, ports) for `coll` on `comm` ("RING" for the
+    RING family, whose schedule ignores both)."""
+    if comm.family.get(coll) == "RING":
+        return "RING", 1
     return comm.algo.get(coll, DEFAULT_VARIANT[coll]), comm.ports
 
 
@@ -213,7 +224,10 @@ def allowed_arms(config, valid=None):
 
 def apply_arm(comm, arm):
     coll, v, ports, seg = arm
-    comm.set_algo(coll, v)
+    if v == "RING":
+        comm.set_algo(coll, DEFAULT_VARIANT[coll], "RING")
+    else:
+        comm.set_algo(coll, v)
     comm.set_ports(ports)
     comm.set_segment(seg)
 
@@ -221,13 +235,14 @@ def apply_arm(comm, arm):
 # ------------------------------------------------------------ data sampling
 P_GRID = sorted({int(round(2 ** (k / 4.0))) for k in range(8, 49)} | {6, 12, 24, 48, 96, 384})
 # reduce_scatter / allgather schedules move every block separately
-# (P^2 log P moves); planning beyond 1024 ranks takes tens of seconds.
-MAX_P_VECTOR = 1024
+# (P^2 log P moves: 4.2 M at P = 2048, 16.8 M at P = 4096, where one
+# variant takes 15-23 s to plan and prove); they are sampled up to 2048.
+MAX_P_VECTOR = 2048
 
 
 def sample_configs(n, seed, max_total_bytes=2 << 30):
     """Calls: op 60/20/20 allreduce/reduce_scatter/allgather, P log-uniform
-    on a grid over [4, 4096] ([4, 1024] for the vector collectives),
+    on a grid over [4, 4096] ([4, 2048] for the vector collectives),
     per-rank message log-uniform 32 B..256 MiB (capped so P x message <=
     max_total_bytes), int32 or float32, one in three on a 2-D or 3-D torus
     when P is a power of two >= 16."""
@@ -279,14 +294,23 @@ def time_arm(comm, coll, send, recv, count, code, stream, reps=3, target_us=300.
     return float(np.median(ts))
 
 
-def measure(configs, reps=3, time_budget_s=None, log=None):
+def measure(configs, reps=3, time_budget_s=None, log=None, planners=None):
     """Measures every valid arm of every call on the GPU with the STEPS
-    engine (time_arm), and the busiest link's bytes from the engine's device link accounting.  Calls
-    are grouped by torus so each communicator (and its proof cache) serves
-    many calls.  Returns (configs measured, X [n, IN_DIM], T_us [n, NARMS],
-    L_bytes [n, NARMS], valid [n, NARMS]) in the order of `configs`; arms
-    the engine refuses are invalid.  Stops early, keeping whole calls, once
-    time_budget_s passes (the measured calls are then a subset)."""
+    engine (time_arm), and the busiest link's bytes from the engine's device
+    link accounting.  Returns (configs measured, X [n, IN_DIM], T_us
+    [n, NARMS], L_bytes [n, NARMS], valid [n, NARMS]) in the order of
+    `configs`; arms the engine refuses are invalid.  Stops early, keeping
+    whole calls, once time_budget_s passes (the measured calls are then a
+    subset).
+
+    Planning and proving a call's schedules is host work that takes longer
+    than timing them, so `planners` worker threads (default: the host's
+    cores less two, at most 16) each take the next call, build its
+    communicator and prove every statically valid arm (the planner releases
+    the interpreter lock), while this thread times the prepared calls one
+    at a time on the GPU: timings never overlap each other."""
+    import queue
+    import threading
     import time
 
     import torch
@@ -294,62 +318,98 @@ def measure(configs, reps=3, time_budget_s=None, log=None):
     import bine_trees_fugaku_b200 as bine
 
     stream = torch.cuda.current_stream()
-    keys = sorted({(c["P"], tuple(c["dims"])) for c in configs})
-    perm = np.random.default_rng(0).permutation(len(keys))  # a budget stop keeps every P range
-    group = {k: int(perm[j]) for j, k in enumerate(keys)}
-    order = sorted(range(len(configs)), key=lambda i: (group[(configs[i]["P"], tuple(configs[i]["dims"]))], i))
-    cfgs, X, T, Lb, done = [], [], [], [], []
+    planners = planners or max(1, min(16, (os.cpu_count() or 4) - 2))
     t_start = time.time()
-    comm, comm_key = None, None
-    for i in order:
-        if time_budget_s and time.time() - t_start > time_budget_s:
-            break
-        cfg = configs[i]
-        coll, P, count, es, dims = cfg["coll"], cfg["P"], cfg["count"], cfg["es"], cfg["dims"]
-        if (P, tuple(dims)) != comm_key:
-            if comm is not None:
-                comm.close()
+    ready = queue.Queue(maxsize=2 * planners)
+    lock = threading.Lock()
+    state = {"next": 0, "stop": False}
+
+    def over_budget():
+        return time_budget_s is not None and time.time() - t_start > time_budget_s
+
+    def planner():
+        while True:
+            with lock:
+                if state["stop"] or over_budget() or state["next"] >= len(configs):
+                    break
+                i = state["next"]
+                state["next"] += 1
+            cfg = configs[i]
+            coll, P, count, dims = cfg["coll"], cfg["P"], cfg["count"], cfg["dims"]
             comm = bine.Comm(P, dims if len(dims) > 1 else None)
             comm.set_engine("steps")
+            ok = []
+            for a, arm in enumerate(ARMS):
+                if not statically_valid(arm, coll, P, count, dims):
+                    continue
+                try:
+                    apply_arm(comm, arm)
+                    comm.plan_verify(coll, count)  # plans and proves once; run() reuses both
+                    ok.append(a)
+                except bine.BineError:
+                    continue
+            ready.put((i, comm, ok))
+        ready.put(None)
+
+    threads = [threading.Thread(target=planner, daemon=True) for _ in range(planners)]
+    for t in threads:
+        t.start()
+    rows = {}
+    finished = 0
+    try:
+        while finished < planners:
+            item = ready.get()
+            if item is None:
+                finished += 1
+                continue
+            i, comm, ok = item
+            cfg = configs[i]
+            coll, P, count, es, dims = cfg["coll"], cfg["P"], cfg["count"], cfg["es"], cfg["dims"]
             comm.set_stream(stream)
-            comm_key = (P, tuple(dims))
-        se, re = bine.row_counts(coll, count, P)
-        dtype = torch.int32 if cfg["dtype"] == "int32" else torch.float32
-        code = bine.INT32 if cfg["dtype"] == "int32" else bine.FLOAT
-        send = torch.ones((P, se), dtype=dtype, device="cuda")
-        recv = torch.zeros((P, re), dtype=dtype, device="cuda")
-        links = torch.zeros(P * len(dims) * 2, dtype=torch.int64, device="cuda")
-        t_row = np.full(NARMS, np.nan)
-        l_row = np.full(NARMS, np.nan)
-        for a, arm in enumerate(ARMS):
-            if not statically_valid(arm, coll, P, count, dims):
-                continue
+            se, re = bine.row_counts(coll, count, P)
+            dtype = torch.int32 if cfg["dtype"] == "int32" else torch.float32
+            code = bine.INT32 if cfg["dtype"] == "int32" else bine.FLOAT
+            send = torch.ones((P, se), dtype=dtype, device="cuda")
+            recv = torch.zeros((P, re), dtype=dtype, device="cuda")
+            links = torch.zeros(P * len(dims) * 2, dtype=torch.int64, device="cuda")
+            t_row = np.full(NARMS, np.nan)
+            l_row = np.full(NARMS, np.nan)
+            for a in ok:
+                arm = ARMS[a]
+                try:
+                    apply_arm(comm, arm)
+                    comm.run(coll, send, recv, count, code)  # uploads the device tables once
+                    comm.synchronize()
+                except bine.BineError:
+                    continue
+                t_row[a] = time_arm(comm, coll, send, recv, count, code, stream, reps)
+                comm.link_bytes(coll, count, code, links)
+                l_row[a] = float(links.max().item())
+            del send, recv, links
+            comm.close()
+            rows[i] = (t_row, l_row)
+            if log and len(rows) % 500 == 0:
+                log(f"measured {len(rows)}/{len(configs)} calls in {time.time() - t_start:.0f} s")
+    finally:
+        with lock:
+            state["stop"] = True
+        # Drain so that planners blocked on a full queue can finish.
+        alive = [t for t in threads if t.is_alive()]
+        while alive:
             try:
-                apply_arm(comm, arm)
-                comm.run(coll, send, recv, count, code)  # plans, proves and uploads once
-                comm.synchronize()
-            except bine.BineError:
-                continue
-            t_row[a] = time_arm(comm, coll, send, recv, count, code, stream, reps)
-            comm.link_bytes(coll, count, code, links)
-            l_row[a] = float(links.max().item())
-        del send, recv, links
-        cfgs.append(cfg)
-        done.append(i)
-        X.append(features(coll, P, count, es, dims))
-        T.append(t_row)
-        Lb.append(l_row)
-        if log and len(cfgs) % 50 == 0:
-            log(f"measured {len(cfgs)}/{len(configs)} calls in {time.time() - t_start:.0f} s (P={P})")
-    if comm is not None:
-        comm.close()
-    # Back to the callers' order (measurement ran grouped by torus).
-    back = sorted(range(len(cfgs)), key=lambda k: done[k])
-    cfgs = [cfgs[k] for k in back]
-    X, T, Lb = [X[k] for k in back], [T[k] for k in back], [Lb[k] for k in back]
-    T = np.array(T).reshape(-1, NARMS)
-    Lb = np.array(Lb).reshape(-1, NARMS)
-    return cfgs, np.array(X, np.float32).reshape(-1, IN_DIM), T, Lb, ~np.isnan(T)
+                item = ready.get(timeout=0.1)
+                if item is not None:
+                    item[1].close()
+            except queue.Empty:
+                pass
+            alive = [t for t in threads if t.is_alive()]
+    done = sorted(rows)
+    cfgs = [configs[i] for i in done]
+    T = np.array([rows[i][0] for i in done]).reshape(-1, NARMS)
+    Lb = np.array([rows[i][1] for i in done]).reshape(-1, NARMS)
+    X = np.array([features(c["coll"], c["P"], c["count"], c["es"], c["dims"]) for c in cfgs],
+                 np.float32).reshape(-1, IN_DIM)
+    return cfgs, X, T, Lb, ~np.isnan(T)
 
 
 # ------------------------------------------------------------- the model
@@ -565,7 +625,10 @@ class Picker:
         if keep is not None:
             # The caller's own schedule, restored whatever the outcome; with
             # no arm of the arm space it must at least run as it is.
-            comm.set_algo(coll, keep[0])
+            if keep[0] == "RING":
+                comm.set_algo(coll, DEFAULT_VARIANT[coll], "RING")
+            else:
+                comm.set_algo(coll, keep[0])
             comm.set_ports(keep[1])
             if not cands:
                 comm.plan_verify(coll, count)

@@ -96,11 +96,12 @@ enum { BINE_DISTANCE_INCREASING = 0, BINE_DISTANCE_DECREASING = 1, BINE_DISTANCE
  *   STEPS: one persistent kernel that executes the reference's schedule step
  *     by step (the message pattern of the MPI layer, as device loads and
  *     stores), with a bounded grid-wide barrier between steps;
- *   PIPELINED: the same schedule and moves as STEPS, cut into segments that
- *     each start as soon as the segments they read and overwrite are done,
- *     with no barrier between steps: steps overlap segment by segment and
- *     ports proceed independently (the device analogue of the uTofu layer's
+ *   PIPELINED: the same schedule as STEPS, cut into segments that each
+ *     start as soon as the segments they read and overwrite are done, with
+ *     no barrier between steps: steps overlap segment by segment and ports
+ *     proceed independently (the device analogue of the uTofu layer's
  *     per-port threads and segmented transfers, lib/libbine_common.cc:1741-1879).
+ *     By default several levels run as one pass (bine_comm_set_fusion).
  *     Results equal the STEPS engine's, float32 included. */
 enum { BINE_ENGINE_FUSED = 0, BINE_ENGINE_STEPS = 1, BINE_ENGINE_PIPELINED = 2 };
 
@@ -142,8 +143,8 @@ int bine_comm_set_engine(bine_comm_t comm, int engine);
 int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes);
 
 /* Level fusion for the PIPELINED engine: `levels` consecutive levels of the
- * reference's schedule per pass (1, the default: every level on its own, as
- * the STEPS engine runs them).  Within a pass, values that one step hands to
+ * reference's schedule per pass (1: every level on its own, as the STEPS
+ * engine runs them; 0, the default: chosen per collective, below).  Within a pass, values that one step hands to
  * the next (partial sums, staged messages) stay in registers; a pass writes
  * only what a later pass reads or what is a result, and a copy several ranks
  * receive from one rank is read once.  A write that would overwrite what its
@@ -152,8 +153,10 @@ int bine_comm_set_segment(bine_comm_t comm, long long segment_bytes);
  * element that is read later or is a result holds, at its own position or
  * in its slot, what the reference's buffers hold after that step.  No
  * counterpart in the reference.  0 chooses the levels per pass for each
- * collective (allreduce and reduce 3, reduce_scatter and bcast 4, allgather,
- * scatter and gather 6, alltoall 10). */
+ * collective (allreduce, reduce_scatter and reduce 6; allgather, bcast,
+ * scatter and gather 12; alltoall 13) and runs schedules of more than 2^20
+ * moves level by level: planning a fused schedule costs about 4 us per move
+ * on the host, once per call shape. */
 int bine_comm_set_fusion(bine_comm_t comm, int levels);
 int bine_comm_set_float_order(bine_comm_t comm, int order);
 

@@ -59,7 +59,7 @@ def test_engine_matches_reference(case, engine):
     x = case_input(case)
     root = case.get("root", 0)
     segment = 256 if engine.endswith("seg256") else 0  # many small segments, level dependencies
-    fusion = int(engine.split("fuse")[1].split("-")[0]) if "fuse" in engine else 1  # levels per pass
+    fusion = int(engine.split("-fuse")[1].split("-")[0]) if "-fuse" in engine else 1  # levels per pass
     engine = engine.split("-")[0]
     comm = make_comm(case["P"], case["coll"], case["variant"], case.get("dims"), case.get("ports", 1),
                      case.get("family", "BINE"), case.get("distance"), engine)

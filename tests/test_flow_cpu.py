@@ -28,6 +28,7 @@ def make_comm(case, segment=0):
     comm.set_ports(case.get("ports", 1))
     comm.set_algo(case["coll"], case["variant"], case.get("family", "BINE"), case.get("distance"))
     comm.set_segment(segment)
+    comm.set_fusion(1)  # the level-by-level plan (fused plans: tests/test_fusion_cpu.py)
     return comm
 
 

@@ -231,11 +231,11 @@ def test_fused_dataflow_plan_orders_every_conflict_and_matches_reference(case):
 
 def test_automatic_fusion_uses_the_per_collective_levels():
     """bine_comm_set_fusion(0): each collective takes its own levels per pass
-    (allreduce and reduce 3, reduce_scatter and bcast 4, allgather, scatter
-    and gather 6, alltoall 10); the dataflow plan is that fused plan."""
-    table = {"allreduce": ("B", 3), "reduce_scatter": ("VEC_HALVING_CONT_PERMUTE", 4),
-             "allgather": ("VEC_DOUBLING_CONT_PERMUTE", 6), "bcast": ("BINOMIAL_TREE", 4),
-             "reduce": ("BINOMIAL_TREE", 3), "alltoall": ("LOG", 10)}
+    (allreduce, reduce_scatter and reduce 6; allgather, bcast, scatter and
+    gather 12; alltoall 13); the dataflow plan is that fused plan."""
+    table = {"allreduce": ("B", 6), "reduce_scatter": ("VEC_HALVING_CONT_PERMUTE", 6),
+             "allgather": ("VEC_DOUBLING_CONT_PERMUTE", 12), "bcast": ("BINOMIAL_TREE", 12),
+             "reduce": ("BINOMIAL_TREE", 6), "alltoall": ("LOG", 13)}
     for coll, (variant, levels) in table.items():
         count = 16 * 9 + 1 if coll in ("allreduce", "bcast", "reduce") else 5
         auto = bine.Comm(16)

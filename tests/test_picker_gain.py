@@ -1,12 +1,14 @@
 """The learned picker against exhaustive search and the fixed rule, on the
-committed measurements (tests/golden/picker_dataset.npz: 6,000 sampled
-calls in two batches, every valid arm timed on a B200 with the STEPS engine,
-made by `python bench.py --suite picker`) and the committed weights trained
-on the 80 % of calls outside its `test` split.
+committed measurements (tests/golden/picker_dataset.npz: 13,588 sampled
+calls, every valid arm timed on a B200 with the STEPS engine by
+`python bench.py --suite picker`) and the committed weights trained on the
+calls outside its `test` split (2,895 held-out calls, 2,213 of them with a
+valid arm).
 
 The CPU test evaluates the weights with the float64 reference of the MLP
 (oracle/mlp_ref.py, bf16 rounding at the kernels' points); the GPU test
-runs the same weights through bine_mlp and the runtime Picker."""
+runs the same weights through the fused ensemble kernel and the runtime
+Picker."""
 import json
 import os
 
@@ -19,10 +21,10 @@ from oracle import mlp_ref
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DATASET = os.path.join(HERE, "golden", "picker_dataset.npz")
-# The committed dataset: 3,000 sampled calls (bench.py --suite picker
-# --picker-n 3000), then 3,000 more with another seed merged in
-# (--picker-data <first> --picker-n 3000 --picker-seed 12), every valid arm
-# timed on a B200 with the STEPS engine.
+# The committed dataset: 6,000 calls measured over the first 66 arms (the
+# RING arms unmeasured, hence invalid, for them), 5,790 calls over all 69
+# arms (its held-out fifth and a half: the `test` split) and 1,798 more for
+# training, merged and trained with --picker-data ... --picker-n 0.
 
 
 def load():
@@ -38,14 +40,16 @@ def cpu_predict(X):
 
 
 def check_gain(ev):
-    # Learned picks land within 5 % of the measured optimum on most
-    # held-out calls, far more often than the fixed rule, and are faster
-    # than the fixed rule on average; the model's three best arms, timed,
-    # hold an arm within 5 % of the optimum on >= 95 % of the calls.
-    assert ev["held_out_calls"] >= 900
-    assert ev["pick_within_5pct_of_optimum"] >= 0.89
+    # The stated target is 95 % of pure picks within 5 % of exhaustive
+    # search.  Measured: 93.4 % (the misses concentrate on the integer
+    # allreduce, whose 15 arms the picker may all choose from; the re-timing
+    # noise ceiling is 98.3 %).  The model's three best arms, timed
+    # (Picker.tune), meet the target with 99.1 %.  Learned picks are faster
+    # than the fixed rule, which lands within 5 % on 56 % of the calls.
+    assert ev["held_out_calls"] >= 2200
+    assert ev["pick_within_5pct_of_optimum"] >= 0.93
     assert ev["pick_within_5pct_of_optimum"] >= ev["fixed_rule_within_5pct_of_optimum"] + 0.3
-    assert ev["pick_time_over_optimum_geomean"] <= 1.03
+    assert ev["pick_time_over_optimum_geomean"] <= 1.02
     assert ev["shortlist3_within_5pct_of_optimum"] >= 0.95
     assert ev["speedup_vs_fixed_rule_geomean"] >= 1.2
     assert ev["link_bytes_over_minimum_geomean"] <= 1.01
@@ -60,7 +64,8 @@ def test_dataset_is_consistent():
         assert np.allclose(X[i], pk.features(c["coll"], c["P"], c["count"], c["es"], c["dims"]))
         for a in np.nonzero(valid[i])[0]:
             assert pk.statically_valid(pk.ARMS[a], c["coll"], c["P"], c["count"], c["dims"])
-    assert len(set(te.tolist())) == len(te) == len(cfgs) // 5 and te.max() < len(cfgs)
+    # Held out: half of the 5,790 calls measured over all 69 arms.
+    assert len(set(te.tolist())) == len(te) == 5790 // 2 and 6000 <= te.min() and te.max() < 6000 + 5790
 
 
 def test_learned_picks_beat_the_fixed_rule_on_held_out_calls():
