@@ -51,10 +51,11 @@ def configure(args):
         WORKLOAD = (f"Bine allreduce (variant B, 1 port, 1-D ring), P={P_RANKS} virtual ranks, {COUNT} {args.dtype} "
                     f"per rank, MPI_SUM, {args.engine} engine"
                     + (f" ({args.fusion or 'automatic'} levels per pass)" if args.engine == "pipelined" else "")
-                    + f", {args.order} float order"
+                    + (f", {args.order} float order" if args.dtype == "float" else "")
                     + (f", {args.tree_split} lanes per vector" if args.tree_split else "") + " (profiling variant)")
 METRIC = "virtual-rank Bine allreduce GB/s"
 WORKLOAD = "Bine allreduce (variant B, 1 port, 1-D ring), P=256 virtual ranks, 1,048,576 int32 (4 MiB) per rank, MPI_SUM"
+DEFAULT_WORKLOAD = WORKLOAD
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "allreduce_fused_p256_4MiB_int32.txt")
 
 
@@ -313,19 +314,24 @@ def run_engine_arm(args):
             cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     peak, peak_kind = peaks()
+    default = WORKLOAD == DEFAULT_WORKLOAD
+    half = P_RANKS * COUNT * ES
+    l2_note = (f"inputs {half / 2**20:.0f} MiB and outputs {half / 2**20:.0f} MiB "
+               + ("exceed the 126 MB L2; no flush" if half > 126e6 else
+                  "fit the 126 MB L2 between steps (no flush): a cache-resident profiling variant"))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32" if args.dtype == "int32" else "float32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "P": P_RANKS, "count_per_rank": COUNT, "variant": "B", "ports": 1,
-                       "engine": "fused", "parallelism": f"replicas{world}",
-                       "l2": "inputs 1 GiB and outputs 1 GiB exceed the 126 MB L2; no flush"},
+                       "engine": args.engine, "parallelism": f"replicas{world}", "l2": l2_note},
             "roofline": {"bound": "hbm", "achieved": per_launch_gbs, "peak": peak, "unit": "GB/s",
-                         "frac": per_launch_gbs / peak, "traffic": profiled_traffic(),
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch from the "
-                                           "committed ncu capture (" + os.path.relpath(PROFILE_SUMMARY, ROOT) +
-                                           "), not measured in this run",
+                         "frac": per_launch_gbs / peak, "traffic": profiled_traffic() if default else None,
+                         "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum per launch from the "
+                                            "committed ncu capture (" + os.path.relpath(PROFILE_SUMMARY, ROOT) +
+                                            "), not measured in this run") if default else
+                                           "no committed capture of this profiling variant",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "algorithmic_bytes_per_launch": ALGO_BYTES},
             "cpu_baseline": cpu,

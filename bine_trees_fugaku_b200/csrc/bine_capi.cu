@@ -559,6 +559,24 @@ int fusion_levels(bine_comm_t c, int coll, const Schedule* s = nullptr) {
     return kAutoFusion[coll];
 }
 
+// Blocks of k_flow_fused resident on the device at once: the fused plan
+// cuts each pass into a whole multiple of this many items of equal traffic,
+// so that a pass runs in whole waves.
+int fused_resident_blocks(bine_comm_t c, int es) {
+    int per_sm = 0;
+    cudaError_t e;
+    switch (es) {
+        case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_flow_fused<int8_t>, dev::kFlowThreads, 0); break;
+        case 8: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_flow_fused<int64_t>, dev::kFlowThreads, 0); break;
+        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_flow_fused<int32_t>, dev::kFlowThreads, 0);
+    }
+    if (e != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = kFlowItemsPerSm;
+    }
+    return per_sm * c->num_sms;
+}
+
 int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFused>* out) {
     std::shared_ptr<Schedule> sch;
     int rc0 = get_schedule(c, k, &sch);
@@ -602,9 +620,12 @@ int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFu
             }
         }
     FlowPlan fp;
-    const int64_t piece = c->segment_bytes > 0 ? std::max<int64_t>(16, c->segment_bytes / es) : 0;
+    // Pieces of at most kFlowMaxItemBytes keep every item below 2^31 bytes,
+    // the kernel's 32-bit unit counts.
+    const int64_t piece =
+        c->segment_bytes > 0 ? std::max<int64_t>(16, std::min<int64_t>(c->segment_bytes, kFlowMaxItemBytes) / es) : 0;
     build_flow_fused(fs, c->P, piece, std::max<int64_t>(1, 4096 / es), kFlowMaxItemBytes / es,
-                     kFlowItemsPerSm * c->num_sms, dev::kFusedPieces, &fp);
+                     fused_resident_blocks(c, es), dev::kFusedPieces, &fp);
     auto d = std::make_shared<DevFused>();
     d->tmp_elems = fs.tmp_elems;
     d->npasses = (int)fs.passes.size();

@@ -984,6 +984,11 @@ __global__ void __launch_bounds__(kFlowThreads, kFlowBlocksPerSm) k_flow(StepBuf
 // program on a four-entry register stack in the order of the original
 // levels' additions, and stores the value to every destination; the loads
 // come before the stores, so a move may update its own elements in place.
+// Items of copies only (one leaf per program: the gather and alltoall
+// passes) move eight 16-byte units per thread and round, other items one
+// unit with all its leaves in flight.  Two blocks of 256 threads per SM
+// (at most 128 registers): the planner cuts each pass into a whole multiple
+// of the resident blocks' count of equal-traffic items.
 struct FusedMoveDev {
     int64_t n;
     int32_t leaf_begin, nleaves, dst_begin, ndst;
@@ -1000,17 +1005,17 @@ struct FusedDstDev {
 };
 constexpr int kFuseLeaves = 8;
 constexpr int kFuseDsts = 8;
-constexpr int kFusedPieces = 64;  // pieces per item
+constexpr int kFusedPieces = 256;  // pieces per item, at most one per thread
 
-// Postfix evaluation on a shift-register stack (s0 is the top): a leaf
-// pushes, each addition pops the top two and pushes their sum.  IEEE and
-// wrapping integer addition are commutative, so only the tree's shape
-// matters, and it is the program's.
-template <typename V, typename Add>
+// Postfix evaluation of at most L leaves on a shift-register stack (s0 is
+// the top): a leaf pushes, each addition pops the top two and pushes their
+// sum.  IEEE and wrapping integer addition are commutative, so only the
+// tree's shape matters, and it is the program's.
+template <int L, typename V, typename Add>
 __device__ __forceinline__ V fused_eval(const V* v, const unsigned char* adds, int nl, Add add) {
     V s0 = v[0], s1 = v[0], s2 = v[0], s3 = v[0];
 #pragma unroll
-    for (int j = 1; j < kFuseLeaves; j++) {
+    for (int j = 1; j < L; j++) {
         if (j < nl) {
             s3 = s2;
             s2 = s1;
@@ -1029,8 +1034,121 @@ __device__ __forceinline__ V fused_eval(const V* v, const unsigned char* adds, i
     return s0;
 }
 
+// Per-item tables of k_flow_fused: every piece's leaf and destination
+// addresses, its evaluation program, and block scans of its 16-byte units
+// and of its element units (an unaligned head and tail, or the whole piece
+// when its rows are not mutually 16-byte aligned).  The planner keeps an
+// item below 2^31 elements, so unit counts fit 32 bits.
+struct FusedItemSmem {
+    int pref[kFusedPieces + 1];   // first 16-byte unit of each piece
+    int epref[kFusedPieces + 1];  // first element unit of each piece
+    const char* leaf[kFusedPieces][kFuseLeaves];
+    char* dst[kFusedPieces][kFuseDsts];
+    long long start[kFusedPieces], n[kFusedPieces];
+    int nvec[kFusedPieces], lb[kFusedPieces], db[kFusedPieces];
+    unsigned char adds[kFusedPieces][kFuseLeaves];
+    unsigned char head[kFusedPieces], nl[kFusedPieces], nd[kFusedPieces];
+    long long warp_sum[kFlowThreads / 32];
+    int item, ok, maxnl;
+    unsigned target;
+};
+
+// Last piece of the item whose units (prefix table pref) start at or
+// before unit u; cur is the guess.
+__device__ __forceinline__ int fused_piece(const int* pref, int u, int np, int cur) {
+    if (u >= pref[cur] && u < pref[cur + 1]) return cur;
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pref[mid] <= u) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The 16-byte units of an item whose programs have at most L leaves (L = 1:
+// copies; L = 2: single additions): U units per thread and round, every
+// unit's loads issued before the round's stores.  Units of one item touch
+// disjoint elements apart from a move's in-place reads of its own elements,
+// so the order of rounds and units does not matter.
+template <typename T, int U, int L>
+__device__ __forceinline__ void fused_units_narrow(const FusedItemSmem& S, int tid, int total, int np) {
+    static_assert(L == 1 || L == 2, "narrow programs only");
+    constexpr int es = sizeof(T);
+    int cur = 0;
+    for (int u0 = tid; u0 < total; u0 += U * kFlowThreads) {
+        uint4 v[U][L];
+        int pc[U], off[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const int u = u0 + k * kFlowThreads;
+            pc[k] = -1;
+            off[k] = 0;
+            if (u < total) {
+                cur = fused_piece(S.pref, u, np, cur);
+                pc[k] = cur;
+                off[k] = S.head[cur] * es + (u - S.pref[cur]) * 16;
+                v[k][0] = ld_plain(S.leaf[cur][0] + off[k]);
+                if (L == 2 && S.nl[cur] == 2) v[k][L - 1] = ld_plain(S.leaf[cur][L - 1] + off[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            if (pc[k] < 0) continue;
+            const int p = pc[k];
+            const uint4 val = (L == 2 && S.nl[p] == 2) ? vadd<T>(v[k][0], v[k][L - 1]) : v[k][0];
+            const int nd = S.nd[p];
+#pragma unroll
+            for (int j = 0; j < kFuseDsts; j++)
+                if (j < nd) *(uint4*)(S.dst[p][j] + off[k]) = val;
+        }
+    }
+}
+
+// The 16-byte units of any item: one unit per thread and round, its leaves
+// loaded together.
 template <typename T>
-__global__ void __launch_bounds__(kFlowThreads) k_flow_fused(StepBufs B, const FusedMoveDev* __restrict__ moves,
+__device__ __forceinline__ void fused_units_wide(const FusedItemSmem& S, int tid, int total, int np) {
+    constexpr int es = sizeof(T);
+    int cur = 0;
+    for (int u = tid; u < total; u += kFlowThreads) {
+        cur = fused_piece(S.pref, u, np, cur);
+        const int off = S.head[cur] * es + (u - S.pref[cur]) * 16;
+        const int nl = S.nl[cur], nd = S.nd[cur];
+        uint4 v[kFuseLeaves];
+#pragma unroll
+        for (int j = 0; j < kFuseLeaves; j++)
+            if (j < nl) v[j] = ld_plain(S.leaf[cur][j] + off);
+        const uint4 val = fused_eval<kFuseLeaves>(v, S.adds[cur], nl, [](uint4 x, uint4 y) { return vadd<T>(x, y); });
+#pragma unroll
+        for (int j = 0; j < kFuseDsts; j++)
+            if (j < nd) *(uint4*)(S.dst[cur][j] + off) = val;
+    }
+}
+
+// The element units of an item: a piece's unaligned head, its tail after
+// the 16-byte body, or all of a piece without one.
+template <typename T>
+__device__ __forceinline__ void fused_elements(const FusedItemSmem& S, int tid, int total, int np) {
+    constexpr int per_vec = 16 / sizeof(T);
+    int cur = 0;
+    for (int u = tid; u < total; u += kFlowThreads) {
+        cur = fused_piece(S.epref, u, np, cur);
+        const long long r = u - S.epref[cur];
+        const long long e = r < S.head[cur] ? r : r + (long long)S.nvec[cur] * per_vec;
+        const int nl = S.nl[cur], nd = S.nd[cur];
+        T w[kFuseLeaves];
+#pragma unroll
+        for (int j = 0; j < kFuseLeaves; j++)
+            if (j < nl) w[j] = *((volatile const T*)S.leaf[cur][j] + e);
+        const T val = fused_eval<kFuseLeaves>(w, S.adds[cur], nl, [](T x, T y) { return add_exact<T>(x, y); });
+#pragma unroll
+        for (int j = 0; j < kFuseDsts; j++)
+            if (j < nd) *((T*)S.dst[cur][j] + e) = val;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kFlowThreads, 2) k_flow_fused(StepBufs B, const FusedMoveDev* __restrict__ moves,
                                                             const FusedLeafDev* __restrict__ leaves,
                                                             const FusedDstDev* __restrict__ dsts,
                                                             const StepChunk* __restrict__ pieces,
@@ -1039,60 +1157,74 @@ __global__ void __launch_bounds__(kFlowThreads) k_flow_fused(StepBufs B, const F
                                                             const int* __restrict__ level_items, int nlevels,
                                                             unsigned* done, unsigned* ctl, int* status,
                                                             unsigned long long timeout_ns, unsigned extra) {
-    __shared__ long long s_pref[kFusedPieces + 1];
-    __shared__ const char* s_leaf[kFusedPieces][kFuseLeaves];
-    __shared__ char* s_dst[kFusedPieces][kFuseDsts];
-    __shared__ unsigned char s_adds[kFusedPieces][kFuseLeaves];
-    __shared__ long long s_nvec[kFusedPieces];
-    __shared__ unsigned char s_head[kFusedPieces], s_nl[kFusedPieces], s_nd[kFusedPieces];
-    __shared__ long long s_warp[kFlowThreads / 32];
-    __shared__ int s_item, s_ok;
-    __shared__ unsigned s_target;
+    __shared__ FusedItemSmem S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         const unsigned t = ld_acquire(&ctl[2]) + 1u;
-        s_target = t == 0 ? 1u : t;
+        S.target = t == 0 ? 1u : t;
     }
     __syncthreads();
-    const unsigned target = s_target;
+    const unsigned target = S.target;
     constexpr long long es = sizeof(T);
+    constexpr int kSlots = kFuseLeaves + kFuseDsts;
     for (;;) {
-        if (tid == 0) s_item = *(volatile int*)status == kStepOk ? (int)atomicAdd(&ctl[0], 1u) : nitems;
+        if (tid == 0) {
+            S.item = *(volatile int*)status == kStepOk ? (int)atomicAdd(&ctl[0], 1u) : nitems;
+            S.maxnl = 1;
+        }
         __syncthreads();
-        const int i = s_item;
+        const int i = S.item;
         if (i >= nitems) break;
         const FlowItem it = items[i];
         const int np = it.pend - it.pbeg;  // at most kFusedPieces (the planner's bound)
-        long long units = 0;
+        // The item's tables in three rounds of independent loads, all before
+        // the dependency wait: pieces and moves, then every leaf and
+        // destination address, then each piece's vector body and units.
         if (tid < np) {
             const StepChunk ch = pieces[it.pbeg + tid];
             const FusedMoveDev m = moves[ch.move];
-            uintptr_t mis = 0, first = 0;
-            for (int j = 0; j < m.nleaves; j++) {
-                const FusedLeafDev lf = leaves[m.leaf_begin + j];
-                const char* a = B.base[lf.buf] + (long long)lf.rank * B.stride[lf.buf] + (lf.off + ch.start) * es;
-                s_leaf[tid][j] = a;
-                s_adds[tid][j] = lf.adds;
-                if (j == 0) first = (uintptr_t)a;
-                mis |= (uintptr_t)a ^ first;
+            S.start[tid] = ch.start;
+            S.n[tid] = ch.n;
+            S.lb[tid] = m.leaf_begin;
+            S.db[tid] = m.dst_begin;
+            S.nl[tid] = (unsigned char)m.nleaves;
+            S.nd[tid] = (unsigned char)m.ndst;
+            atomicMax(&S.maxnl, m.nleaves);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int e = tid; e < np * kSlots; e += kFlowThreads) {
+            const int p = e / kSlots, j = e % kSlots;
+            if (j < kFuseLeaves) {
+                if (j < S.nl[p]) {
+                    const FusedLeafDev lf = leaves[S.lb[p] + j];
+                    S.leaf[p][j] =
+                        B.base[lf.buf] + (long long)lf.rank * B.stride[lf.buf] + (lf.off + S.start[p]) * es;
+                    S.adds[p][j] = lf.adds;
+                }
+            } else if (j - kFuseLeaves < S.nd[p]) {
+                const FusedDstDev d = dsts[S.db[p] + j - kFuseLeaves];
+                S.dst[p][j - kFuseLeaves] =
+                    B.base[d.buf] + (long long)d.rank * B.stride[d.buf] + (d.off + S.start[p]) * es;
             }
-            for (int j = 0; j < m.ndst; j++) {
-                const FusedDstDev d = dsts[m.dst_begin + j];
-                char* p = B.base[d.buf] + (long long)d.rank * B.stride[d.buf] + (d.off + ch.start) * es;
-                s_dst[tid][j] = p;
-                mis |= (uintptr_t)p ^ first;
-            }
-            const long long n = ch.n;
-            long long head = n, nvec = 0;
+        }
+        __syncthreads();
+        // Both unit counts in one scan: element units in the high half.
+        long long units = 0;
+        if (tid < np) {
+            const uintptr_t first = (uintptr_t)S.leaf[tid][0];
+            uintptr_t mis = 0;
+            for (int j = 1; j < S.nl[tid]; j++) mis |= (uintptr_t)S.leaf[tid][j] ^ first;
+            for (int j = 0; j < S.nd[tid]; j++) mis |= (uintptr_t)S.dst[tid][j] ^ first;
+            const long long n = S.n[tid];
+            long long head = 0, nvec = 0;
             if ((mis & 15) == 0) {
                 head = min((long long)((16 - (first & 15)) & 15) / es, n);
                 nvec = (n - head) * es / 16;
             }
-            units = n - nvec * (16 / es) + nvec;
-            s_nvec[tid] = nvec;
-            s_head[tid] = (unsigned char)min(head, 255ll);
-            s_nl[tid] = (unsigned char)m.nleaves;
-            s_nd[tid] = (unsigned char)m.ndst;
+            units = ((n - nvec * (16 / es)) << 32) | nvec;
+            S.nvec[tid] = (int)nvec;
+            S.head[tid] = (unsigned char)head;
         }
         long long inc = units;
 #pragma unroll
@@ -1100,57 +1232,29 @@ __global__ void __launch_bounds__(kFlowThreads) k_flow_fused(StepBufs B, const F
             const long long v = __shfl_up_sync(0xffffffffu, inc, o);
             if (lane >= o) inc += v;
         }
-        if (lane == 31) s_warp[warp] = inc;
+        if (lane == 31) S.warp_sum[warp] = inc;
         __syncthreads();
         long long before = 0;
-        for (int w = 0; w < warp; w++) before += s_warp[w];
-        if (tid < kFusedPieces) s_pref[tid + 1] = before + inc;
-        if (tid == 0) s_pref[0] = 0;
+        for (int w = 0; w < warp; w++) before += S.warp_sum[w];
+        S.pref[tid + 1] = (int)((before + inc) & 0xffffffffll);
+        S.epref[tid + 1] = (int)((before + inc) >> 32);
+        if (tid == 0) S.pref[0] = S.epref[0] = 0;
         if (warp == 0) {
             bool ok = true;
             for (int d = it.dbeg + lane; d < it.dend && ok; d += 32)
                 ok = flow_wait(deps[d], done, ctl, level_items, target, extra, status, timeout_ns);
             ok = __all_sync(0xffffffffu, ok);
-            if (lane == 0) s_ok = ok;
+            if (lane == 0) S.ok = ok;
         }
         __syncthreads();
-        if (!s_ok) break;
-        const long long total = s_pref[np];
-        int cur = 0;
-        for (long long u = tid; u < total; u += kFlowThreads) {
-            if (!(u >= s_pref[cur] && u < s_pref[cur + 1])) {
-                int lo = 0, hi = np - 1;  // last piece starting at or before u
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_pref[mid] <= u) lo = mid; else hi = mid - 1;
-                }
-                cur = lo;
-            }
-            const long long r = u - s_pref[cur];
-            const long long head = s_head[cur], nvec = s_nvec[cur];
-            const int nl = s_nl[cur], nd = s_nd[cur];
-            if (r >= head && r < head + nvec) {
-                const long long off = head * es + (r - head) * 16;
-                uint4 v[kFuseLeaves];
-#pragma unroll
-                for (int j = 0; j < kFuseLeaves; j++)
-                    if (j < nl) v[j] = ld_plain(s_leaf[cur][j] + off);
-                const uint4 val = fused_eval(v, s_adds[cur], nl, [](uint4 x, uint4 y) { return vadd<T>(x, y); });
-#pragma unroll
-                for (int j = 0; j < kFuseDsts; j++)
-                    if (j < nd) *(uint4*)(s_dst[cur][j] + off) = val;
-            } else {
-                const long long e = r < head ? r : r - nvec + nvec * (16 / es);
-                T v[kFuseLeaves];
-#pragma unroll
-                for (int j = 0; j < kFuseLeaves; j++)
-                    if (j < nl) v[j] = *((volatile const T*)s_leaf[cur][j] + e);
-                const T val = fused_eval(v, s_adds[cur], nl, [](T x, T y) { return add_exact<T>(x, y); });
-#pragma unroll
-                for (int j = 0; j < kFuseDsts; j++)
-                    if (j < nd) *((T*)s_dst[cur][j] + e) = val;
-            }
-        }
+        if (!S.ok) break;  // a wait expired; the status is recorded
+        const int total = S.pref[np];
+        const int maxnl = S.maxnl;
+        if (maxnl <= 1)
+            fused_units_narrow<T, 8, 1>(S, tid, total, np);
+        else
+            fused_units_wide<T>(S, tid, total, np);
+        if (S.epref[np] > 0) fused_elements<T>(S, tid, S.epref[np], np);
         __syncthreads();
         if (tid == 0) {
             st_release(&done[i], target);

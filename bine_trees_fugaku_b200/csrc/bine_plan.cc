@@ -2008,14 +2008,76 @@ struct FlowAccess {
     bool write;
 };
 
+// Balanced packing of one level (build_flow_fused without a segment size):
+// every element of move m costs weights[m] element accesses (its leaves and
+// destinations).  The level is cut into items of equal access counts, as
+// many as a whole multiple of `target_items` (the kernel's resident blocks)
+// that keeps items at or below 2 * max_item_elems accesses, so that the
+// items of a level run in whole waves.  A move is cut where an item fills,
+// at multiples of min_item_elems from the move's start.
+void pack_balanced(const std::vector<int64_t>& sizes, const std::vector<int32_t>& weights, int32_t first_move,
+                   int level, int64_t min_item_elems, int64_t max_item_elems, int target_items, int max_pieces,
+                   FlowPlan* out, int32_t* nitems) {
+    int64_t level_w = 0;
+    for (size_t m = 0; m < sizes.size(); m++) level_w += sizes[m] * weights[m];
+    const int64_t cap_w = 2 * max_item_elems;
+    const int64_t tw = (int64_t)target_items * cap_w;
+    // Every move opens at most one piece beyond its share of the items, so
+    // goal * (max_pieces - 1) >= moves keeps items within max_pieces.
+    const int64_t tp = (int64_t)target_items * std::max(1, max_pieces - 1);
+    const int64_t waves = std::max<int64_t>({1, (level_w + tw - 1) / tw, ((int64_t)sizes.size() + tp - 1) / tp});
+    // Levels too small for that get items of 2 * min_item_elems accesses.
+    const int64_t goal = std::max<int64_t>(1, std::min(waves * target_items, level_w / (2 * min_item_elems)));
+    // Item k ends where the level's accesses reach (k + 1) / goal of the
+    // total; a move is cut at the multiple of min_item_elems nearest that
+    // boundary.  An item that reaches max_pieces first is continued by a
+    // new item toward the same boundary.
+    auto bound = [&](int64_t k) { return std::max<int64_t>(1, (k + 1) * level_w / goal); };
+    int64_t pos = 0, k = 0;  // accesses placed; boundary of the open item
+    bool full = true;        // the next piece opens a new item
+    *nitems = 0;
+    for (size_t m = 0; m < sizes.size(); m++) {
+        const int64_t mn = sizes[m], w = std::max<int32_t>(1, weights[m]);
+        for (int64_t st = 0; st < mn;) {
+            const bool capped = *nitems > 0 && out->items.back().pend - out->items.back().pbeg >= max_pieces;
+            if (full || capped) {
+                if (full && *nitems > 0) k++;
+                const int32_t p = (int32_t)out->pieces.size();
+                out->items.push_back(FlowItem{p, p, 0, 0, (int32_t)level, 0});
+                ++*nitems;
+                full = false;
+            }
+            const int64_t room = bound(k) - pos;
+            int64_t n = mn - st;
+            if (n * w > room) {
+                n = std::min(n, (room / w + min_item_elems / 2) / min_item_elems * min_item_elems);
+                if (n <= 0) {
+                    if (out->items.back().pend > out->items.back().pbeg) {
+                        full = true;
+                        continue;
+                    }
+                    n = std::min(mn - st, min_item_elems);
+                }
+            }
+            out->pieces.push_back(FlowPiece{first_move + (int32_t)m, 0, st, n});
+            out->items.back().pend++;
+            pos += n * w;
+            st += n;
+            if (pos >= bound(k)) full = true;
+        }
+    }
+}
+
 // The shared core of build_flow and build_flow_fused: `sizes[l]` are the
 // element counts of level l's moves (numbered in level order), and
 // visit(move, start, n, fn) calls fn(rank, buf, offset, n, write) for every
 // row range the elements [start, start + n) of that move read or write.
+// With `weights` (element accesses per element of each move) and no piece
+// size, levels are packed by pack_balanced.
 template <typename Visit>
 void build_flow_impl(const std::vector<std::vector<int64_t>>& sizes, int P, int64_t piece_elems,
                      int64_t min_item_elems, int64_t max_item_elems, int target_items, int max_pieces, Visit visit,
-                     FlowPlan* out) {
+                     FlowPlan* out, const std::vector<std::vector<int32_t>>* weights = nullptr) {
     *out = FlowPlan();
     max_pieces = std::max(1, std::min(max_pieces, kFlowMaxPieces));
     const bool auto_pieces = piece_elems <= 0;
@@ -2027,6 +2089,14 @@ void build_flow_impl(const std::vector<std::vector<int64_t>>& sizes, int P, int6
     std::vector<int32_t> level_first;  // first item of each level
     for (size_t l = 0; l < sizes.size(); l++) {
         level_first.push_back((int32_t)out->items.size());
+        if (weights && auto_pieces) {
+            int32_t nitems = 0;
+            pack_balanced(sizes[l], (*weights)[l], nmoves, (int)l, min_item_elems, max_item_elems, target_items,
+                          max_pieces, out, &nitems);
+            nmoves += (int32_t)sizes[l].size();
+            out->level_items.push_back(nitems);
+            continue;
+        }
         int64_t level_elems = 0;
         for (int64_t n : sizes[l]) level_elems += n;
         int64_t item_elems = std::max(min_item_elems, (level_elems + target_items - 1) / target_items);
@@ -2194,10 +2264,12 @@ void build_flow(const Schedule& s, int P, int64_t piece_elems, int64_t min_item_
 void build_flow_fused(const FusedSchedule& f, int P, int64_t piece_elems, int64_t min_item_elems,
                       int64_t max_item_elems, int target_items, int max_pieces, FlowPlan* out) {
     std::vector<std::vector<int64_t>> sizes(f.passes.size());
+    std::vector<std::vector<int32_t>> weights(f.passes.size());
     std::vector<const FusedMove*> move_of;
     for (size_t l = 0; l < f.passes.size(); l++)
         for (const FusedMove& m : f.passes[l]) {
             sizes[l].push_back(m.n);
+            weights[l].push_back(m.nleaves + m.ndst);
             move_of.push_back(&m);
         }
     build_flow_impl(sizes, P, piece_elems, min_item_elems, max_item_elems, target_items, max_pieces,
@@ -2212,7 +2284,7 @@ void build_flow_fused(const FusedSchedule& f, int P, int64_t piece_elems, int64_
                             fn(d.rank, d.buf, d.off + st, n, true);
                         }
                     },
-                    out);
+                    out, &weights);
 }
 
 }  // namespace bine

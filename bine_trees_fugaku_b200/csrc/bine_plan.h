@@ -257,7 +257,10 @@ bool fuse_schedule(const Schedule& s, int P, int depth, const std::vector<bool>&
                    std::string* err);
 
 // build_flow for a fused schedule: pieces index fused moves (pass order);
-// reads are every leaf, writes every destination.
+// reads are every leaf, writes every destination.  Without a piece size,
+// each pass is cut into items of equal traffic (leaves + destinations per
+// element), as many as a whole multiple of `target_items`: the kernel's
+// resident blocks, so that a pass runs in whole waves.
 void build_flow_fused(const FusedSchedule& f, int P, int64_t piece_elems, int64_t min_item_elems,
                       int64_t max_item_elems, int target_items, int max_pieces, FlowPlan* out);
 

@@ -97,7 +97,7 @@ def check_plan(mv, lv, dv, pieces, items, deps):
     cross-pass element conflict."""
     cover = [[] for _ in range(len(mv))]
     for i, (pb, pe, db, de, lev) in enumerate(items.tolist()):
-        assert 0 < pe - pb <= 64
+        assert 0 < pe - pb <= 256
         for p in range(pb, pe):
             m, s, c = pieces[p].tolist()
             assert mv[m][0] == lev and c > 0
