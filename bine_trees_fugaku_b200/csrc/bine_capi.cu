@@ -113,6 +113,9 @@ static_assert(sizeof(FusedMove) == sizeof(dev::FusedMoveDev), "fused move layout
 static_assert(sizeof(FusedLeaf) == sizeof(dev::FusedLeafDev), "fused leaf layouts differ");
 static_assert(sizeof(FusedDst) == sizeof(dev::FusedDstDev), "fused destination layouts differ");
 static_assert(dev::kFuseLeaves == kFuseMaxLeaves && dev::kFuseDsts == kFuseMaxDsts, "fusion bounds differ");
+static_assert((int)BINE_COLL_ALLREDUCE == kAllreduce && (int)BINE_COLL_REDUCE_SCATTER == kReduceScatter &&
+                  (int)BINE_COLL_ALLGATHER == kAllgather && (int)BINE_COLL_GATHER == kGather,
+              "collective codes differ");
 
 // Device copy of the exact reduction trees of one call.
 struct DevTrees {
@@ -607,8 +610,8 @@ int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFu
                 if (lf.rank < 0 || lf.rank >= c->P || lf.buf > kBufTmp || lf.off < 0 || lf.off + m.n > rows[lf.buf] ||
                     (j == 0 && lf.adds != 0) || lf.adds > 3)
                     return fail(BINE_ERR_INTERNAL, "fusion produced a leaf outside its buffer row");
+                maxd = std::max(maxd, depth + 1);  // the leaf is pushed before its additions
                 depth += 1 - lf.adds;
-                maxd = std::max(maxd, depth);
                 if (depth < 1) return fail(BINE_ERR_INTERNAL, "fusion produced a malformed program");
             }
             if (depth != 1 || maxd > kFuseMaxDepth) return fail(BINE_ERR_INTERNAL, "fusion produced a malformed program");
@@ -2386,12 +2389,13 @@ int bine_link_bytes(bine_comm_t comm, bine_coll_t coll, long count, bine_datatyp
     for (int p = 0; p < comm->ports; p++) mirrored |= mirrored_port(p, t.ndims);
     int kind = -1;
     if (all_p2 && cf.family != kFamilyRing && (cf.family == kFamilyBine || !mirrored)) {
-        if (coll == kAllreduce && (cf.variant == kArB || cf.variant == kArBCoalesce) && cf.distance == kIncreasing &&
+        const int cl = (int)coll;
+        if (cl == kAllreduce && (cf.variant == kArB || cf.variant == kArBCoalesce) && cf.distance == kIncreasing &&
             count >= (long)comm->ports * t.size)
             kind = 0;
-        else if (coll == kAllreduce && cf.variant == kArL)
+        else if (cl == kAllreduce && cf.variant == kArL)
             kind = 1;
-        else if (coll == kAllgather && cf.variant == kAgContPermute && cf.distance == kDecreasing)
+        else if (cl == kAllgather && cf.variant == kAgContPermute && cf.distance == kDecreasing)
             kind = 2;
     }
     if (kind >= 0) {

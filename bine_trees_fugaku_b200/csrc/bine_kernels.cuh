@@ -1006,6 +1006,7 @@ struct FusedDstDev {
 constexpr int kFuseLeaves = 8;
 constexpr int kFuseDsts = 8;
 constexpr int kFusedPieces = 256;  // pieces per item, at most one per thread
+static_assert(kFusedPieces <= kFlowThreads, "one thread per piece of an item");
 
 // Postfix evaluation of at most L leaves on a shift-register stack (s0 is
 // the top): a leaf pushes, each addition pops the top two and pushes their
@@ -1236,8 +1237,10 @@ __global__ void __launch_bounds__(kFlowThreads, 2) k_flow_fused(StepBufs B, cons
         __syncthreads();
         long long before = 0;
         for (int w = 0; w < warp; w++) before += S.warp_sum[w];
-        S.pref[tid + 1] = (int)((before + inc) & 0xffffffffll);
-        S.epref[tid + 1] = (int)((before + inc) >> 32);
+        if (tid < kFusedPieces) {
+            S.pref[tid + 1] = (int)((before + inc) & 0xffffffffll);
+            S.epref[tid + 1] = (int)((before + inc) >> 32);
+        }
         if (tid == 0) S.pref[0] = S.epref[0] = 0;
         if (warp == 0) {
             bool ok = true;

@@ -206,28 +206,40 @@ __device__ __forceinline__ void mma_bf16_16816(float* d, const uint32_t* a, cons
 
 // One layer for 16 rows: out[16][N] = act[16][K] W^T + bias, then GELU into
 // the next activation buffer (hidden) or fp32 into `outf` (last layer).
-// Warp w owns the n-tile w (8 columns; N <= 8 * warps).  It first loads all
-// of that tile's weight fragments for the whole K (at most 16 k-steps, two
-// 32-bit registers each), so the layer costs one round of L2 latency rather
-// than one per k-step, then runs its mma chain from the activations in
-// shared memory.
-__device__ __forceinline__ void ens_layer(const bf16* __restrict__ act, int lda, int K, const bf16* __restrict__ W,
-                                          const float* __restrict__ bias, int N, bf16* next, int ldn, float* outf,
-                                          int ldo) {
+// Warp w owns the n-tile w (8 columns; N <= 8 * warps).  Its weight
+// fragments for the whole K (at most 16 k-steps, two 32-bit registers each)
+// and its two bias values are loaded in one round (ens_fetch), and the
+// kernel issues the next layer's round as soon as this layer's mma chain
+// has consumed the fragments, so that the L2 latency of layer l + 1 runs
+// under layer l's epilogue and block barrier.
+struct EnsFrag {
+    uint32_t b[16][2];
+    float b0, b1;
+};
+
+__device__ __forceinline__ void ens_fetch(EnsFrag& f, int K, const bf16* __restrict__ W, const float* __restrict__ bias,
+                                          int N) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int j = warp;
-    if (j * 8 >= N) return;
+    if (warp * 8 >= N) return;
     const int ksteps = K / 16;
-    uint32_t b[16][2];
-    const bf16* wr = W + (size_t)(j * 8 + g) * K + 2 * t;
+    const bf16* wr = W + (size_t)(warp * 8 + g) * K + 2 * t;
 #pragma unroll
     for (int kk = 0; kk < 16; kk++)
         if (kk < ksteps) {
-            b[kk][0] = __ldg((const unsigned int*)(wr + kk * 16));
-            b[kk][1] = __ldg((const unsigned int*)(wr + kk * 16 + 8));
+            f.b[kk][0] = __ldg((const unsigned int*)(wr + kk * 16));
+            f.b[kk][1] = __ldg((const unsigned int*)(wr + kk * 16 + 8));
         }
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const int c = warp * 8 + 2 * t;
+    f.b0 = __ldg(bias + c);
+    f.b1 = __ldg(bias + c + 1);
+}
+
+// The mma chain of one layer from fragments already in registers.
+__device__ __forceinline__ void ens_mma(float* acc, const bf16* __restrict__ act, int lda, int K, const EnsFrag& f) {
+    const int lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int ksteps = K / 16;
 #pragma unroll
     for (int kk = 0; kk < 16; kk++)
         if (kk < ksteps) {
@@ -237,10 +249,16 @@ __device__ __forceinline__ void ens_layer(const bf16* __restrict__ act, int lda,
             a[1] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 2 * t);
             a[2] = *(const uint32_t*)(act + g * lda + k0 + 8 + 2 * t);
             a[3] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 8 + 2 * t);
-            mma_bf16_16816(acc, a, b[kk]);
+            mma_bf16_16816(acc, a, f.b[kk]);
         }
-    const int c = j * 8 + 2 * t;
-    const float b0 = bias[c], b1 = bias[c + 1];
+}
+
+// Bias and GELU into the next activation buffer, or fp32 output.
+__device__ __forceinline__ void ens_epilogue(const float* acc, float b0, float b1, bf16* next, int ldn, float* outf,
+                                             int ldo) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int c = warp * 8 + 2 * t;
     const float v[4] = {acc[0] + b0, acc[1] + b1, acc[2] + b0, acc[3] + b1};
     if (next) {
         *(__nv_bfloat162*)(next + g * ldn + c) = __floats2bfloat162_rn(gelu(v[0]), gelu(v[1]));
@@ -262,16 +280,28 @@ __global__ void __launch_bounds__(kEnsThreads) k_mlp_ensemble(EnsArgs a) {
     const int model = (int)cluster.block_rank();
     const int row0 = blockIdx.y * 16;
     const EnsModel M = a.m[model];
+    const int dims[5] = {a.din, kEnsH, kEnsH, kEnsH, a.dout};
+    const int warp = threadIdx.x >> 5;
+    EnsFrag f;
+    ens_fetch(f, dims[0], M.wb + a.woff[0], M.w + a.boff[0], dims[1]);
     for (int i = threadIdx.x; i < 16 * a.din; i += kEnsThreads) {
         const int r = i / a.din, k = i % a.din;
         s_act[0][r * kLd + k] = __float2bfloat16(a.x[(size_t)(row0 + r) * a.din + k]);
     }
     __syncthreads();
-    const int dims[5] = {a.din, kEnsH, kEnsH, kEnsH, a.dout};
+#pragma unroll 1
     for (int l = 0; l < 4; l++) {
         const bf16* in = s_act[l & 1];
         bf16* nxt = l < 3 ? s_act[(l + 1) & 1] : nullptr;
-        ens_layer(in, kLd, dims[l], M.wb + a.woff[l], M.w + a.boff[l], dims[l + 1], nxt, kLd, s_out, a.dout);
+        if (warp * 8 < dims[l + 1]) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            ens_mma(acc, in, kLd, dims[l], f);
+            const float b0 = f.b0, b1 = f.b1;
+            if (l < 3) ens_fetch(f, dims[l + 1], M.wb + a.woff[l + 1], M.w + a.boff[l + 1], dims[l + 2]);
+            ens_epilogue(acc, b0, b1, nxt, kLd, s_out, a.dout);
+        } else if (l < 3) {
+            ens_fetch(f, dims[l + 1], M.wb + a.woff[l + 1], M.w + a.boff[l + 1], dims[l + 2]);
+        }
         __syncthreads();
     }
     cluster.sync();
