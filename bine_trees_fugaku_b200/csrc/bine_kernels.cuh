@@ -981,14 +981,15 @@ __global__ void __launch_bounds__(kFlowThreads, kFlowBlocksPerSm) k_flow(StepBuf
 // program over at most kFuseLeaves state elements, written to at most
 // kFuseDsts destinations.  Each unit (a 16-byte vector, or an element at a
 // piece's unaligned head and tail) loads all of its leaves, evaluates the
-// program on a four-entry register stack in the order of the original
-// levels' additions, and stores the value to every destination; the loads
+// program on a four-entry stack (the top in registers, the rest in shared
+// memory for 16-byte units) in the order of the original levels'
+// additions, and stores the value to every destination; the loads
 // come before the stores, so a move may update its own elements in place.
 // Items of copies only (one leaf per program: the gather and alltoall
-// passes) move eight 16-byte units per thread and round, other items one
-// unit with all its leaves in flight.  Two blocks of 256 threads per SM
-// (at most 128 registers): the planner cuts each pass into a whole multiple
-// of the resident blocks' count of equal-traffic items.
+// passes) move four 16-byte units per thread and round, other items one
+// unit with all its leaves in flight.  Three blocks of 256 threads per SM
+// (80 registers): the planner cuts each pass into a whole multiple of the
+// resident blocks' count of equal-traffic items.
 struct FusedMoveDev {
     int64_t n;
     int32_t leaf_begin, nleaves, dst_begin, ndst;
@@ -1005,7 +1006,7 @@ struct FusedDstDev {
 };
 constexpr int kFuseLeaves = 8;
 constexpr int kFuseDsts = 8;
-constexpr int kFusedPieces = 256;  // pieces per item, at most one per thread
+constexpr int kFusedPieces = 128;  // pieces per item, at most one per thread
 static_assert(kFusedPieces <= kFlowThreads, "one thread per piece of an item");
 
 // Postfix evaluation of at most L leaves on a shift-register stack (s0 is
@@ -1049,6 +1050,9 @@ struct FusedItemSmem {
     int nvec[kFusedPieces], lb[kFusedPieces], db[kFusedPieces];
     unsigned char adds[kFusedPieces][kFuseLeaves];
     unsigned char head[kFusedPieces], nl[kFusedPieces], nd[kFusedPieces];
+    uint4 stk[3][kFlowThreads];  // evaluation stack below the top (depth <= 4), per thread
+    char* base[3];               // the launch's buffer rows (StepBufs), read from shared memory
+    long long stride[3];
     long long warp_sum[kFlowThreads / 32];
     int item, ok, maxnl;
     unsigned target;
@@ -1106,9 +1110,11 @@ __device__ __forceinline__ void fused_units_narrow(const FusedItemSmem& S, int t
 }
 
 // The 16-byte units of any item: one unit per thread and round, its leaves
-// loaded together.
+// loaded together, the program evaluated with the entries below the top of
+// its stack in this thread's column of S.stk (registers would cost the
+// third block per SM).
 template <typename T>
-__device__ __forceinline__ void fused_units_wide(const FusedItemSmem& S, int tid, int total, int np) {
+__device__ __forceinline__ void fused_units_wide(FusedItemSmem& S, int tid, int total, int np) {
     constexpr int es = sizeof(T);
     int cur = 0;
     for (int u = tid; u < total; u += kFlowThreads) {
@@ -1119,10 +1125,18 @@ __device__ __forceinline__ void fused_units_wide(const FusedItemSmem& S, int tid
 #pragma unroll
         for (int j = 0; j < kFuseLeaves; j++)
             if (j < nl) v[j] = ld_plain(S.leaf[cur][j] + off);
-        const uint4 val = fused_eval<kFuseLeaves>(v, S.adds[cur], nl, [](uint4 x, uint4 y) { return vadd<T>(x, y); });
+        uint4 top = v[0];
+        int sp = 0;
+#pragma unroll
+        for (int j = 1; j < kFuseLeaves; j++)
+            if (j < nl) {
+                S.stk[sp++][tid] = top;
+                top = v[j];
+                for (int a = S.adds[cur][j]; a > 0; a--) top = vadd<T>(S.stk[--sp][tid], top);
+            }
 #pragma unroll
         for (int j = 0; j < kFuseDsts; j++)
-            if (j < nd) *(uint4*)(S.dst[cur][j] + off) = val;
+            if (j < nd) *(uint4*)(S.dst[cur][j] + off) = top;
     }
 }
 
@@ -1149,7 +1163,7 @@ __device__ __forceinline__ void fused_elements(const FusedItemSmem& S, int tid, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kFlowThreads, 2) k_flow_fused(StepBufs B, const FusedMoveDev* __restrict__ moves,
+__global__ void __launch_bounds__(kFlowThreads, 3) k_flow_fused(StepBufs B, const FusedMoveDev* __restrict__ moves,
                                                             const FusedLeafDev* __restrict__ leaves,
                                                             const FusedDstDev* __restrict__ dsts,
                                                             const StepChunk* __restrict__ pieces,
@@ -1163,6 +1177,10 @@ __global__ void __launch_bounds__(kFlowThreads, 2) k_flow_fused(StepBufs B, cons
     if (tid == 0) {
         const unsigned t = ld_acquire(&ctl[2]) + 1u;
         S.target = t == 0 ? 1u : t;
+    }
+    if (tid < 3) {
+        S.base[tid] = B.base[tid];
+        S.stride[tid] = B.stride[tid];
     }
     __syncthreads();
     const unsigned target = S.target;
@@ -1200,13 +1218,13 @@ __global__ void __launch_bounds__(kFlowThreads, 2) k_flow_fused(StepBufs B, cons
                 if (j < S.nl[p]) {
                     const FusedLeafDev lf = leaves[S.lb[p] + j];
                     S.leaf[p][j] =
-                        B.base[lf.buf] + (long long)lf.rank * B.stride[lf.buf] + (lf.off + S.start[p]) * es;
+                        S.base[lf.buf] + (long long)lf.rank * S.stride[lf.buf] + (lf.off + S.start[p]) * es;
                     S.adds[p][j] = lf.adds;
                 }
             } else if (j - kFuseLeaves < S.nd[p]) {
                 const FusedDstDev d = dsts[S.db[p] + j - kFuseLeaves];
                 S.dst[p][j - kFuseLeaves] =
-                    B.base[d.buf] + (long long)d.rank * B.stride[d.buf] + (d.off + S.start[p]) * es;
+                    S.base[d.buf] + (long long)d.rank * S.stride[d.buf] + (d.off + S.start[p]) * es;
             }
         }
         __syncthreads();
@@ -1254,7 +1272,7 @@ __global__ void __launch_bounds__(kFlowThreads, 2) k_flow_fused(StepBufs B, cons
         const int total = S.pref[np];
         const int maxnl = S.maxnl;
         if (maxnl <= 1)
-            fused_units_narrow<T, 8, 1>(S, tid, total, np);
+            fused_units_narrow<T, 4, 1>(S, tid, total, np);
         else
             fused_units_wide<T>(S, tid, total, np);
         if (S.epref[np] > 0) fused_elements<T>(S, tid, S.epref[np], np);
