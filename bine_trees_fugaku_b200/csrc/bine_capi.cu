@@ -8,6 +8,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -151,14 +152,35 @@ struct DevTrees {
     int nstiles = 0;
     int smax_prog_len = 0;
     int sdepth = 0;  // deepest stack of any part or combine program
+    // Row-aligned split form (k_tree_flat): when set, `stiles` holds its
+    // tiles (absolute element starts on the row's grid) instead of
+    // per-segment ones.
+    bool flat = false;
+    int64_t* fbody = nullptr;
+    uint16_t* franks = nullptr;
+    uint16_t* franks_t = nullptr;
+    uint8_t* fadds = nullptr;
+    int* fparts = nullptr;
+    dev::TreeComb* fcomb = nullptr;
+    int* fassign = nullptr;
+    dev::FlatEdge* fedges = nullptr;
+    int fpitch = 0, flen = 0, fmax_ns = 0, fnq = 0;
+    std::vector<dev::FlatEdge> h_fedges;
+    // Edges (k_tree_edges): their own split plan, cut into
+    // dev::kEdgeParts parts, with its entry-major rank table.
+    uint8_t* feadds = nullptr;
+    int* feparts = nullptr;
+    dev::TreeComb* fecomb = nullptr;
+    uint16_t* feranks_t = nullptr;
+    int felen = 0, fedepth = 0, nfedges = 0;
     // Host copies of the tile lists and segment offsets, for column windows.
     std::vector<dev::TreeTile> h_tiles, h_stiles, h_rtiles, h_htiles, h_atiles;
     std::vector<int64_t> h_seg_off;
     // Per window width: every window's clipped tiles of each list, with
     // per-window begin indices (list k: tiles[k] + begin[k][i]).
     struct Windows {
-        dev::TreeTile* tiles[5] = {};
-        std::vector<int> begin[5];
+        dev::TreeTile* tiles[6] = {};
+        std::vector<int> begin[6];
     };
     std::map<long long, Windows> windows;
     ~DevTrees() {
@@ -178,6 +200,18 @@ struct DevTrees {
         cudaFree(uparts);
         cudaFree(ucomb);
         cudaFree(stiles);
+        cudaFree(fbody);
+        cudaFree(franks);
+        cudaFree(franks_t);
+        cudaFree(fedges);
+        cudaFree(feadds);
+        cudaFree(feparts);
+        cudaFree(fecomb);
+        cudaFree(feranks_t);
+        cudaFree(fadds);
+        cudaFree(fparts);
+        cudaFree(fcomb);
+        cudaFree(fassign);
     }
 };
 
@@ -668,6 +702,145 @@ int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFu
     return BINE_SUCCESS;
 }
 
+// Tables of the row-aligned split form (k_tree_flat), built when every
+// segment with a vector body sends its result to every rank and its split
+// program has the same additions, part offsets and combine program as the
+// others, with every leaf at shift 0 (allreduce).  Segments are indexed in
+// the order of their bodies.  Row tiles are the output row's own groups of
+// `W` elements that hold some body, each with the first body it touches and
+// how many (at most kFlatSegs, or the form is not used).  Edges are the
+// vectors between two adjacent bodies that straddle their segments'
+// boundary (evaluated with their own split plan `se`, when it has one
+// shape too), and the head and tail pieces the edges cover are listed in
+// `covered` (segment, first element in it) for the element kernel to skip.
+// `sassign` is the split plan's per-segment warp assignment.
+struct FlatTables {
+    std::vector<int64_t> body;
+    std::vector<uint16_t> ranks, ranks_t;
+    std::vector<uint8_t> adds;
+    std::vector<int> parts, assign;
+    std::vector<dev::TreeComb> comb;
+    std::vector<dev::FlatEdge> edges;
+    std::vector<dev::TreeTile> tiles;
+    // The edges' split plan (dev::kEdgeParts parts) and rank table.
+    std::vector<uint8_t> eadds;
+    std::vector<int> eparts;
+    std::vector<dev::TreeComb> ecomb;
+    std::vector<uint16_t> eranks_t;
+    int edepth = 0;
+    std::set<std::pair<int32_t, int64_t>> covered;
+    int pitch = 0, len = 0, max_ns = 0, nq = 0;
+};
+
+bool flat_tables(const TreePlan& tp, const SplitTrees& st, const SplitTrees* se, int K, int KP,
+                 const std::vector<int>& sassign, const std::vector<int64_t>& body_lo,
+                 const std::vector<int64_t>& body_hi, int64_t W, int L, int P, FlatTables* f) {
+    if (P > 65536) return false;
+    std::vector<int> order;
+    for (size_t i = 0; i < tp.segs.size(); i++)
+        if (body_lo[i] < body_hi[i]) order.push_back((int)i);
+    if (order.empty()) return false;
+    std::sort(order.begin(), order.end(),
+              [&](int a, int b) { return tp.segs[a].off + body_lo[a] < tp.segs[b].off + body_lo[b]; });
+    const int f0 = order[0];
+    const int32_t* p0 = &st.parts[(size_t)f0 * (KP + 1)];
+    const int len = p0[KP] - p0[0];
+    const int NA = KP + K + 1;
+    for (int i : order) {
+        if (tp.segs[i].rank >= 0) return false;
+        const int32_t* po = &st.parts[(size_t)i * (KP + 1)];
+        for (int j = 0; j <= KP; j++)
+            if (po[j] - po[0] != p0[j] - p0[0]) return false;
+        for (int j = 0; j < KP; j++)
+            if (st.comb[(size_t)i * KP + j] != st.comb[(size_t)f0 * KP + j]) return false;
+        for (int j = 0; j < NA; j++)
+            if (sassign[(size_t)i * NA + j] != sassign[(size_t)f0 * NA + j]) return false;
+        for (int k = 0; k < len; k++) {
+            const ProgEntry& e = st.prog[po[0] + k];
+            const ProgEntry& e0 = st.prog[p0[0] + k];
+            if (e.shift != 0 || e.adds != e0.adds || e.adds < 0 || e.adds > 255 || e.rank < 0 || e.rank >= P)
+                return false;
+        }
+    }
+    const size_t nq = order.size();
+    f->nq = (int)nq;
+    f->len = (len + 15) / 16 * 16;
+    f->pitch = (len + 7) / 8 * 8;
+    f->adds.assign(f->len, 0);
+    for (int k = 0; k < len; k++) f->adds[k] = (uint8_t)st.prog[p0[0] + k].adds;
+    for (int j = 0; j <= KP; j++) f->parts.push_back(p0[j] - p0[0]);
+    for (int j = 0; j < KP; j++)
+        f->comb.push_back(dev::TreeComb{st.comb[(size_t)f0 * KP + j].first, st.comb[(size_t)f0 * KP + j].second});
+    f->assign.assign(sassign.begin() + (size_t)f0 * NA, sassign.begin() + (size_t)(f0 + 1) * NA);
+    f->ranks.assign(nq * f->pitch, 0);
+    f->ranks_t.assign((size_t)f->pitch * nq, 0);
+    for (size_t q = 0; q < nq; q++) {
+        const int i = order[q];
+        const int32_t* po = &st.parts[(size_t)i * (KP + 1)];
+        for (int k = 0; k < len; k++) {
+            const uint16_t r = (uint16_t)st.prog[po[0] + k].rank;
+            f->ranks[q * f->pitch + k] = r;
+            f->ranks_t[(size_t)k * nq + q] = r;
+        }
+        f->body.push_back(tp.segs[i].off + body_lo[i]);
+        f->body.push_back(tp.segs[i].off + body_hi[i]);
+    }
+    // Edges: one vector between adjacent bodies, cut by the boundary of
+    // their (adjacent) segments; only with an edge split plan of one shape.
+    const int NE = dev::kEdgeParts;
+    bool edges_ok = se != nullptr;
+    const int32_t* e0 = edges_ok ? &se->parts[(size_t)f0 * (NE + 1)] : nullptr;
+    for (size_t q = 0; edges_ok && q < nq; q++) {
+        const int i = order[q];
+        const int32_t* po = &se->parts[(size_t)i * (NE + 1)];
+        for (int j = 0; j <= NE; j++) edges_ok &= po[j] - po[0] == e0[j] - e0[0];
+        for (int j = 0; j < NE; j++) edges_ok &= se->comb[(size_t)i * NE + j] == se->comb[(size_t)f0 * NE + j];
+        for (int k = 0; edges_ok && k < len; k++)
+            edges_ok &= se->prog[po[0] + k].adds == se->prog[e0[0] + k].adds && se->prog[po[0] + k].shift == 0;
+    }
+    if (edges_ok) {
+        f->eadds.assign(f->len, 0);
+        for (int k = 0; k < len; k++) f->eadds[k] = (uint8_t)se->prog[e0[0] + k].adds;
+        for (int j = 0; j <= NE; j++) f->eparts.push_back(e0[j] - e0[0]);
+        for (int j = 0; j < NE; j++)
+            f->ecomb.push_back(dev::TreeComb{se->comb[(size_t)f0 * NE + j].first, se->comb[(size_t)f0 * NE + j].second});
+        f->eranks_t.assign((size_t)f->pitch * nq, 0);
+        for (size_t q = 0; q < nq; q++) {
+            const int32_t* po = &se->parts[(size_t)order[q] * (NE + 1)];
+            for (int k = 0; k < len; k++) f->eranks_t[(size_t)k * nq + q] = (uint16_t)se->prog[po[0] + k].rank;
+        }
+        int cdepth = 1, sp = 0;
+        for (int j = 0; j < NE; j++) {
+            cdepth = std::max(cdepth, ++sp);
+            sp -= f->ecomb[j].adds;
+        }
+        f->edepth = std::max(se->max_depth, cdepth);
+        for (size_t q = 0; q + 1 < nq; q++) {
+            const OutSegment& a = tp.segs[order[q]];
+            const OutSegment& b = tp.segs[order[q + 1]];
+            const int64_t e = f->body[2 * q + 1];
+            if (a.off + a.n != b.off || f->body[2 * q + 2] != e + L || b.off <= e || b.off >= e + L) continue;
+            f->edges.push_back(dev::FlatEdge{e, (int32_t)q, (int32_t)(b.off - e)});
+            f->covered.insert({order[q], body_hi[order[q]]});
+            f->covered.insert({order[q + 1], 0});
+        }
+    }
+    // Row tiles on the row's grid of W elements.
+    const int64_t first = f->body.front() / W * W, last = f->body.back();
+    size_t q = 0;
+    for (int64_t a = first; a < last; a += W) {
+        const int64_t b = a + W;
+        while (q < nq && f->body[2 * q + 1] <= a) q++;
+        size_t r = q;
+        while (r < nq && f->body[2 * r] < b) r++;
+        if (r == q) continue;
+        if (r - q > (size_t)dev::kFlatSegs) return false;
+        f->max_ns = std::max(f->max_ns, (int)(r - q));
+        f->tiles.push_back(dev::TreeTile{(int32_t)q, (int32_t)(r - q), a, W});
+    }
+    return true;
+}
+
 int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTrees>* out) {
     std::shared_ptr<Schedule> s;
     int rc = get_schedule(c, k, &s);
@@ -865,6 +1038,51 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
                 add_tiles(&stiles, (int32_t)i, body_lo[i], body_hi[i], (int64_t)(dev::kThreads / K) * L);
             }
             d->split_parts = KP;
+            FlatTables ft;
+            SplitTrees se;
+            std::string serr;
+            const bool have_se = min_leaves >= 2 * dev::kEdgeParts && split_trees(tp, dev::kEdgeParts, &se, &serr) &&
+                                 se.max_depth <= dev::kMaxTreeDepth;
+            if (flat_tables(tp, st, have_se ? &se : nullptr, K, KP, sassign, body_lo, body_hi,
+                            (int64_t)(dev::kThreads / K) * L, (int)L, c->P, &ft)) {
+                cudaError_t g[9];
+                fill(&d->fbody, ft.body, &g[0]);
+                fill(&d->franks, ft.ranks, &g[1]);
+                fill(&d->franks_t, ft.ranks_t, &g[2]);
+                fill(&d->fadds, ft.adds, &g[3]);
+                fill(&d->fparts, ft.parts, &g[4]);
+                fill(&d->fcomb, ft.comb, &g[5]);
+                fill(&d->fassign, ft.assign, &g[6]);
+                fill(&d->fedges, ft.edges, &g[7]);
+                cudaError_t h[4];
+                fill(&d->feadds, ft.eadds, &h[0]);
+                fill(&d->feparts, ft.eparts, &h[1]);
+                fill(&d->fecomb, ft.ecomb, &h[2]);
+                fill(&d->feranks_t, ft.eranks_t, &h[3]);
+                for (cudaError_t x : h)
+                    if (x != cudaSuccess) return fail(BINE_ERR_CUDA, "uploading the row-aligned reduction trees failed");
+                d->nfedges = (int)ft.edges.size();
+                d->felen = ft.len;
+                d->fedepth = ft.edepth;
+                // The element kernel keeps only the pieces no edge covers.
+                std::vector<dev::TreeTile> keep;
+                for (const dev::TreeTile& t : htiles)
+                    if (!ft.covered.count({t.seg, t.start})) keep.push_back(t);
+                cudaFree(d->htiles);
+                d->htiles = nullptr;
+                fill(&d->htiles, keep, &g[8]);
+                for (cudaError_t x : g)
+                    if (x != cudaSuccess) return fail(BINE_ERR_CUDA, "uploading the row-aligned reduction trees failed");
+                d->nhtiles = (int)keep.size();
+                d->h_htiles = keep;
+                d->flat = true;
+                d->fpitch = ft.pitch;
+                d->flen = ft.len;
+                d->fmax_ns = ft.max_ns;
+                d->fnq = ft.nq;
+                d->h_fedges = ft.edges;
+                stiles = std::move(ft.tiles);
+            }
             std::vector<dev::TreeEntry> sprog;
             for (const ProgEntry& e : st.prog) sprog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
             cudaError_t f1, f2, f3, f4, f5, f6;
@@ -1050,18 +1268,103 @@ int launch_tree_split(bine_comm_t c, const DevTrees& d, const char* in, long lon
     return BINE_SUCCESS;
 }
 
+// Arguments and dynamic shared memory of the row-aligned kernels: the
+// common additions, the ranks of up to `fmax_ns` segments (row tiles only),
+// then the evaluation stacks when they fit.
+struct FlatLaunch {
+    dev::FlatArgs a;
+    size_t smem;
+    bool in_smem;
+};
+FlatLaunch flat_launch(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
+                       const dev::TreeTile* tiles, int ntiles, bool rows) {
+    const size_t adds = (size_t)d.flen, ranks = rows ? ((size_t)d.fmax_ns * d.fpitch * 2 + 15) / 16 * 16 : 0;
+    const size_t stack = (size_t)std::max(1, d.sdepth) * dev::kThreads * 16;
+    FlatLaunch f;
+    f.in_smem = stack <= 64 * 1024 && adds + ranks + stack <= 200 * 1024;
+    f.smem = adds + ranks + (f.in_smem ? stack : 0);
+    dev::FlatArgs& a = f.a;
+    a.in = in;
+    a.in_stride = ist;
+    a.out = out;
+    a.out_stride = ost;
+    a.P = c->P;
+    a.body = d.fbody;
+    a.ranks = d.franks;
+    a.ranks_t = d.franks_t;
+    a.pitch = d.fpitch;
+    a.nq = d.fnq;
+    a.adds = d.fadds;
+    a.len = d.flen;
+    a.parts = d.fparts;
+    a.comb = d.fcomb;
+    a.assign = d.fassign;
+    a.edges = d.fedges;
+    a.tiles = tiles;
+    a.ntiles = ntiles;
+    a.nparts = d.split_parts;
+    a.ranks_off = (int)(adds / 16);
+    a.stack_off = (int)((adds + ranks) / 16);
+    return f;
+}
+
+template <typename T, int K>
+int launch_tree_flat(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
+                     const dev::TreeTile* ftiles, int nftiles) {
+    if (nftiles == 0) return BINE_SUCCESS;
+    const FlatLaunch f = flat_launch(c, d, in, ist, out, ost, ftiles, nftiles, true);
+    auto kern = f.in_smem ? dev::k_tree_flat<T, K, true> : dev::k_tree_flat<T, K, false>;
+    unsigned g = 0;
+    int rc = launch_tree_kernel(c, kern, f.smem, nftiles, &g);
+    if (rc) return rc;
+    kern<<<g, dev::kThreads, f.smem, c->stream>>>(f.a);
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
+template <typename T>
+int launch_tree_edges(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
+                      int first, int nedges, cudaStream_t s) {
+    if (nedges == 0) return BINE_SUCCESS;
+    const size_t adds = (size_t)d.felen, stack = (size_t)std::max(1, d.fedepth) * dev::kThreads * 16;
+    const bool in_smem = stack <= 64 * 1024 && adds + stack <= 200 * 1024;
+    const size_t smem = adds + (in_smem ? stack : 0);
+    dev::FlatArgs a{};
+    a.in = in;
+    a.in_stride = ist;
+    a.out = out;
+    a.out_stride = ost;
+    a.P = c->P;
+    a.ranks_t = d.feranks_t;
+    a.nq = d.fnq;
+    a.adds = d.feadds;
+    a.len = d.felen;
+    a.parts = d.feparts;
+    a.comb = d.fecomb;
+    a.edges = d.fedges + first;
+    a.stack_off = (int)(adds / 16);
+    auto kern = in_smem ? dev::k_tree_edges<T, true> : dev::k_tree_edges<T, false>;
+    unsigned g = 0;
+    int rc = launch_tree_kernel(c, kern, smem, 2LL * ((nedges + 31) / 32), &g);
+    if (rc) return rc;
+    kern<<<g, dev::kThreads, smem, s>>>(a, nedges);
+    CUDA_TRY(cudaGetLastError());
+    return BINE_SUCCESS;
+}
+
 // Tile lists of a launch: vector tiles (one-lane and split forms) and
 // element tiles (the remainder, or everything for unaligned layouts).
 struct TileSet {
-    // vector one-lane, vector split, element remainder, short element
-    // pieces, element all
-    const dev::TreeTile* t[5];
-    int n[5];
+    // vector one-lane, vector split (or row-aligned rows), element
+    // remainder, short element pieces, element all, row-aligned edges
+    const dev::TreeTile* t[6];
+    int n[6];
+    int edge0;  // row-aligned edges: the first (list 5 holds no tiles, n[5] counts edges)
 };
 
 TileSet all_tiles(const DevTrees& d) {
-    return TileSet{{d.tiles, d.stiles, d.rtiles, d.htiles, d.atiles},
-                   {d.ntiles, d.nstiles, d.nrtiles, d.nhtiles, d.natiles}};
+    return TileSet{{d.tiles, d.stiles, d.rtiles, d.htiles, d.atiles, nullptr},
+                   {d.ntiles, d.nstiles, d.nrtiles, d.nhtiles, d.natiles, d.nfedges}, 0};
 }
 
 // Evaluates the trees of `d` over the tiles of `ts` (all of them, or one
@@ -1076,12 +1379,17 @@ int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist,
     const bool vec = aligned16(in) && aligned16(out) && ist % 16 == 0 && ost % 16 == 0;
     unsigned g = 0;
     int rc;
-    const bool side = vec && (ts.n[2] > 0 || ts.n[3] > 0);
+    const bool edges = vec && d.flat && ts.n[5] > 0;
+    const bool side = vec && (ts.n[2] > 0 || ts.n[3] > 0 || edges);
     cudaStream_t es = c->stream;
     if (side) {
         CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
         CUDA_TRY(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
         es = c->side;
+        if (edges) {
+            rc = launch_tree_edges<T>(c, d, in, ist, out, ost, ts.edge0, ts.n[5], es);
+            if (rc) return rc;
+        }
         if (ts.n[3] > 0) {
             // The split plan's parts when there is one (its segments index
             // the same output runs), else each whole tree as one part.
@@ -1099,7 +1407,14 @@ int launch_tree(bine_comm_t c, const DevTrees& d, const char* in, long long ist,
             CUDA_TRY(cudaGetLastError());
         }
     }
-    if (vec && d.split_k > 1 && ts.n[1] > 0) {
+    if (vec && d.flat && ts.n[1] > 0) {
+        switch (d.split_k) {
+        case 2: rc = launch_tree_flat<T, 2>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
+        case 4: rc = launch_tree_flat<T, 4>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
+        default: rc = launch_tree_flat<T, 8>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
+        }
+        if (rc) return rc;
+    } else if (vec && d.split_k > 1 && ts.n[1] > 0) {
         switch (d.split_k) {
         case 2: rc = launch_tree_split<T, 2>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
         case 4: rc = launch_tree_split<T, 4>(c, d, in, ist, out, ost, ts.t[1], ts.n[1]); break;
@@ -1441,22 +1756,32 @@ int window_tiles(bine_comm_t c, DevTrees& d, long long W, long long count, const
     std::lock_guard<std::mutex> lk(c->mu);
     auto it = d.windows.find(W);
     if (it == d.windows.end()) {
-        auto clip = [&](const std::vector<dev::TreeTile>& in, long long c0, long long c1,
+        // Tiles hold a segment and a start inside it, except the row-aligned
+        // form's, which hold absolute starts (and a segment range, kept).
+        auto clip = [&](const std::vector<dev::TreeTile>& in, bool absolute, long long c0, long long c1,
                         std::vector<dev::TreeTile>* o) {
             for (const dev::TreeTile& t : in) {
-                const long long lo = d.h_seg_off[t.seg] + t.start, hi = lo + t.n;
+                const long long base = absolute ? 0 : d.h_seg_off[t.seg];
+                const long long lo = base + t.start, hi = lo + t.n;
                 const long long a = std::max(lo, c0), b = std::min(hi, c1);
-                if (a < b) o->push_back(dev::TreeTile{t.seg, 0, a - d.h_seg_off[t.seg], b - a});
+                if (a < b) o->push_back(dev::TreeTile{t.seg, t.pad, a - base, b - a});
             }
         };
         const std::vector<dev::TreeTile>* lists[5] = {&d.h_tiles, &d.h_stiles, &d.h_rtiles, &d.h_htiles,
                                                       &d.h_atiles};
         DevTrees::Windows w;
+        // Row-aligned edges: per window, the first edge at or after its start.
+        for (long long c0 = 0; c0 < count; c0 += W) {
+            int a = 0;
+            while (a < (int)d.h_fedges.size() && d.h_fedges[a].e < c0) a++;
+            w.begin[5].push_back(a);
+        }
+        w.begin[5].push_back((int)d.h_fedges.size());
         for (int k = 0; k < 5; k++) {
             std::vector<dev::TreeTile> v;
             for (long long c0 = 0; c0 < count; c0 += W) {
                 w.begin[k].push_back((int)v.size());
-                clip(*lists[k], c0, std::min(count, c0 + W), &v);
+                clip(*lists[k], k == 1 && d.flat, c0, std::min(count, c0 + W), &v);
             }
             w.begin[k].push_back((int)v.size());
             cudaError_t e;
@@ -1481,6 +1806,9 @@ int launch_tree_window(bine_comm_t c, const DevTrees& d, const DevTrees::Windows
         ts.t[k] = w->tiles[k] + w->begin[k][i];
         ts.n[k] = w->begin[k][i + 1] - w->begin[k][i];
     }
+    ts.t[5] = nullptr;
+    ts.edge0 = w->begin[5][i];
+    ts.n[5] = w->begin[5][i + 1] - w->begin[5][i];
     return launch_tree<T>(c, d, in, ist, out, ost, ts);
 }
 
@@ -2167,6 +2495,23 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms) {
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     comm->barrier_extra = extra;
+    return BINE_SUCCESS;
+}
+
+int bine_debug_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                         int* form, int* lanes) {
+    if (!comm || !form || !lanes) return fail(BINE_ERR_ARG, "null argument");
+    if (datatype != BINE_FLOAT && datatype != BINE_DOUBLE) return fail(BINE_ERR_ARG, "not a floating-point type");
+    if (!is_reduction(coll)) return fail(BINE_ERR_ARG, "not a reduction");
+    if (count <= 0) return fail(BINE_ERR_ARG, "count must be positive");
+    if (root < 0 || root >= comm->P) return fail(BINE_ERR_ARG, "root out of range");
+    int rc = ensure_device(comm);
+    if (rc) return rc;
+    std::shared_ptr<DevTrees> d;
+    rc = get_dev_trees(comm, make_key(comm, coll, count, root), dtype_size(datatype), &d);
+    if (rc) return rc;
+    *lanes = d->split_k;
+    *form = d->flat ? 3 : (d->split_k > 1 && d->nstiles > 0 ? 2 : (d->ntiles > 0 ? 1 : 0));
     return BINE_SUCCESS;
 }
 

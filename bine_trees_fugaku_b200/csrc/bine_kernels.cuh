@@ -441,6 +441,214 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
     }
 }
 
+// Row-aligned form of k_tree_split, for calls whose trees all have one
+// shape.  In allreduce every leaf reads its rank's row at the output's own
+// column, and every segment's tree (one segment per block of the
+// reference's vector) has the same additions: segments differ only in the
+// order of their ranks.  The tiles of k_tree_split start at each segment's
+// first 16-byte boundary; with non-power-of-two P that is an arbitrary
+// 16-byte offset, so every 512-byte warp access straddles five 128-byte
+// lines, and a segment's last tile is mostly empty.  Here tiles follow the
+// output row's own grid of 32-vector groups instead: `tile.start` is a
+// multiple of the tile width (in elements, from the row start), a tile may
+// hold the ends of several segments (`tile.pad` of them from `tile.seg`, in
+// the order of their bodies), and each lane evaluates its own segment's
+// ranks.
+//
+// A vector that straddles two consecutive segments (an "edge": its first
+// `cut` elements end segment q, the rest begin segment q + 1) is evaluated
+// by k_tree_edges, beside this kernel, as a whole 16-byte vector, instead of
+// element by element.  The additions, and so the results, are exactly the
+// trees'.
+//
+//   body[2q], body[2q+1] segment q's vector body [lo, hi), in elements
+//   ranks[q * pitch + k] the rank of entry k of segment q's split program;
+//   ranks_t[k * nq + q] the same, entry-major (edge lanes read consecutive q)
+//   adds[k]             additions after entry k (the same for every segment)
+//   parts, comb, assign the common split plan (as in k_tree_split)
+constexpr int kFlatSegs = 8;  // segments one row tile may touch
+
+struct FlatEdge {  // the vector at element `e`: elements [e, e + cut) in segment q, the rest in q + 1
+    int64_t e;
+    int32_t q, cut;
+};
+
+struct FlatArgs {
+    const char* in;
+    long long in_stride;
+    char* out;
+    long long out_stride;
+    int P;
+    const int64_t* body;
+    const uint16_t* ranks;
+    const uint16_t* ranks_t;
+    int pitch, nq;
+    const uint8_t* adds;
+    int len;  // bytes of `adds`, a multiple of 16
+    const int* parts;
+    const TreeComb* comb;
+    const int* assign;
+    const FlatEdge* edges;
+    const TreeTile* tiles;
+    int ntiles, nparts;
+    int ranks_off, stack_off;  // dynamic shared memory offsets, in 16-byte words
+};
+
+// Evaluates entries [b, b + len) of a program whose additions are
+// `adds` and whose ranks are rk[k * rstep] (1: a row of the shared-memory
+// rank table; nq: a column of the entry-major global table, so that the
+// lanes of an edge tile, which own consecutive segments, read consecutive
+// words), for one 16-byte vector at `base`; loads run kRing entries ahead
+// of the additions.
+template <typename T, bool SMEM, int kRing>
+__device__ __forceinline__ uint4 eval_ranks(const char* __restrict__ base, long long stride, const uint16_t* rk,
+                                            int rstep, const uint8_t* adds, int b, int len, EvalStack<SMEM>& stk) {
+    uint4 top = make_uint4(0, 0, 0, 0);
+    int sp = 0;
+    uint4 ring[kRing];
+#pragma unroll
+    for (int u = 0; u < kRing; u++)
+        if (u < len) ring[u] = ld_stream(base + (long long)rk[(b + u) * rstep] * stride);
+    for (int k0 = 0; k0 < len; k0 += kRing) {
+#pragma unroll
+        for (int u = 0; u < kRing; u++) {
+            const int k = k0 + u;
+            if (k < len) {
+                const uint4 v = ring[u];
+                if (k + kRing < len) ring[u] = ld_stream(base + (long long)rk[(b + k + kRing) * rstep] * stride);
+                if (k > 0) stk.set(sp++, top);
+                top = v;
+                for (int a = adds[b + k]; a > 0; a--) top = vadd<T>(stk.get(--sp), top);
+            }
+        }
+    }
+    return top;
+}
+
+template <typename T, int K, bool SMEM>
+__global__ void __launch_bounds__(kThreads) k_tree_flat(const FlatArgs A) {
+    extern __shared__ uint4 sdyn[];
+    uint8_t* sadds = reinterpret_cast<uint8_t*>(sdyn);
+    uint16_t* sranks = reinterpret_cast<uint16_t*>(sdyn + A.ranks_off);
+    EvalStack<SMEM> stk;
+    stk.init(sdyn + A.stack_off);
+    constexpr int kWarps = kThreads / 32;
+    constexpr int kGroups = kWarps / K;
+    constexpr int KP = 2 * K;
+    __shared__ int spart[KP + 1];
+    __shared__ TreeComb scomb[KP];
+    __shared__ int sasg[KP + K + 1];
+    __shared__ int64_t slo[kFlatSegs], shi[kFlatSegs];
+    __shared__ uint4 partial[kGroups][KP][32];
+    constexpr int L = 16 / sizeof(T);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = warp % K, g = warp / K;
+    const int nparts = A.nparts;
+    // The common plan, once per block.
+    for (int i = threadIdx.x; i < A.len / 16; i += blockDim.x) sdyn[i] = reinterpret_cast<const uint4*>(A.adds)[i];
+    if (threadIdx.x <= nparts) spart[threadIdx.x] = A.parts[threadIdx.x];
+    if (threadIdx.x < nparts) scomb[threadIdx.x] = A.comb[threadIdx.x];
+    if (threadIdx.x < nparts + K + 1) sasg[threadIdx.x] = A.assign[threadIdx.x];
+    const int words = A.pitch / 8;  // 16-byte words of one segment's ranks
+    const uint4* granks = reinterpret_cast<const uint4*>(A.ranks);
+    uint4* sranks4 = reinterpret_cast<uint4*>(sranks);
+    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
+        const TreeTile tile = A.tiles[t];
+        const int s0 = tile.seg, ns = tile.pad;
+        __syncthreads();  // the previous tile's partials and ranks are consumed
+        for (int i = threadIdx.x; i < ns * words; i += blockDim.x) sranks4[i] = granks[(long long)s0 * words + i];
+        if (threadIdx.x < ns) {
+            slo[threadIdx.x] = A.body[2 * (s0 + threadIdx.x)];
+            shi[threadIdx.x] = A.body[2 * (s0 + threadIdx.x) + 1];
+        }
+        __syncthreads();
+        const long long e = tile.start + (long long)(g * 32 + lane) * L;  // first element of the lane's vector
+        int slot = -1;
+        if (e < tile.start + tile.n)
+            for (int q = 0; q < ns; q++)
+                if (e >= slo[q] && e < shi[q]) slot = q;
+        const bool active = slot >= 0;
+        if (active) {
+            const uint16_t* rk = sranks + slot * A.pitch;
+            for (int pi = sasg[nparts + j]; pi < sasg[nparts + j + 1]; pi++) {
+                const int p = sasg[pi];
+                partial[g][p][lane] = eval_ranks<T, SMEM, 4>(A.in + e * (long long)sizeof(T), A.in_stride, rk, 1,
+                                                             sadds, spart[p], spart[p + 1] - spart[p], stk);
+            }
+        }
+        __syncthreads();
+        if (!active) continue;
+        uint4 top = make_uint4(0, 0, 0, 0);
+        int csp = 0;
+        for (int q = 0; q < nparts; q++) {
+            const TreeComb c = scomb[q];
+            if (q > 0) stk.set(csp++, top);
+            top = partial[g][c.part][lane];
+            for (int a = c.adds; a > 0; a--) top = vadd<T>(stk.get(--csp), top);
+        }
+        for (int d = j; d < A.P; d += K)
+            st_stream(A.out + (long long)d * A.out_stride + e * (long long)sizeof(T), top);
+    }
+}
+
+// The edges of the row-aligned form (see above).  Their trees are cut into
+// kEdgeParts subtrees of their own (the edge split plan: `parts`, `comb`,
+// `adds`, and ranks_t in that plan's entry order), so that an edge's
+// critical path is P / kEdgeParts leaves whatever the row tiles' split.
+// Block b owns edges [32 * (b / 2), +32) and segment side b % 2 (0: the
+// segment the edge vector ends, 1: the one it starts); warp w evaluates
+// part w for its lane's edge, the partial sums meet in shared memory, and
+// every lane combines them and stores the elements of its side (the first
+// `cut` elements of the vector, or the rest) to the rows w, w + 8, ...  The
+// two sides of an edge run in neighbouring blocks, so the two halves of its
+// 16-byte vector reach L2 close together.
+constexpr int kEdgeParts = 8;
+
+template <typename T, bool SMEM>
+__global__ void __launch_bounds__(kThreads) k_tree_edges(const FlatArgs A, int nedges) {
+    extern __shared__ uint4 sdyn[];
+    uint8_t* sadds = reinterpret_cast<uint8_t*>(sdyn);
+    EvalStack<SMEM> stk;
+    stk.init(sdyn + A.stack_off);
+    static_assert(kThreads / 32 == kEdgeParts, "one warp per edge part");
+    __shared__ int spart[kEdgeParts + 1];
+    __shared__ TreeComb scomb[kEdgeParts];
+    __shared__ uint4 partial[kEdgeParts][32];
+    constexpr int L = 16 / sizeof(T);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < A.len / 16; i += blockDim.x) sdyn[i] = reinterpret_cast<const uint4*>(A.adds)[i];
+    if (threadIdx.x <= kEdgeParts) spart[threadIdx.x] = A.parts[threadIdx.x];
+    if (threadIdx.x < kEdgeParts) scomb[threadIdx.x] = A.comb[threadIdx.x];
+    const int ngroups = (nedges + 31) / 32;
+    for (int t = blockIdx.x; t < 2 * ngroups; t += gridDim.x) {
+        const int side = t & 1, ei = (t >> 1) * 32 + lane;
+        const bool act = ei < nedges;
+        FlatEdge ed{0, 0, 0};
+        if (act) ed = A.edges[ei];
+        __syncthreads();  // the previous partials are consumed (and the plan staged)
+        if (act)
+            partial[w][lane] = eval_ranks<T, SMEM, 4>(A.in + ed.e * (long long)sizeof(T), A.in_stride,
+                                                      A.ranks_t + ed.q + side, A.nq, sadds, spart[w],
+                                                      spart[w + 1] - spart[w], stk);
+        __syncthreads();
+        if (!act) continue;
+        uint4 top = make_uint4(0, 0, 0, 0);
+        int csp = 0;
+        for (int q = 0; q < kEdgeParts; q++) {
+            const TreeComb c = scomb[q];
+            if (q > 0) stk.set(csp++, top);
+            top = partial[c.part][lane];
+            for (int a = c.adds; a > 0; a--) top = vadd<T>(stk.get(--csp), top);
+        }
+        const T* r = reinterpret_cast<const T*>(&top);
+        const int x0 = side ? ed.cut : 0, x1 = side ? L : ed.cut;
+        for (int d = w; d < A.P; d += kEdgeParts) {
+            T* o = reinterpret_cast<T*>(A.out + (long long)d * A.out_stride + ed.e * (long long)sizeof(T));
+            for (int x = x0; x < x1; x++) o[x] = r[x];
+        }
+    }
+}
+
 // Element form for the short head and tail pieces of segments (fewer
 // elements than one 16-byte vector).  Per tile the block
 //   1. loads every leaf value of the tile's elements into shared memory in

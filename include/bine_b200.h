@@ -276,6 +276,15 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms);
  * faults or hangs. */
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
 
+/* Which kernel evaluates the vector bodies of an exact-order float
+ * reduction on a 16-byte-aligned layout (FUSED engine): *form is 0 (element
+ * kernel only), 1 (one lane per vector), 2 (K lanes per vector, tiles per
+ * segment) or 3 (K lanes per vector, tiles on the row's own grid, for
+ * trees of one shape); *lanes is K.  Plans the call without running it.
+ * No reference counterpart: introspection for tests. */
+int bine_debug_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                         int *form, int *lanes);
+
 /* Lanes that cooperate on one output vector in the exact-order float
  * reduction (1, 2, 4 or 8; 0, the default, chooses per call from the
  * output size).  Results are identical for every setting. */

@@ -124,6 +124,13 @@ def reference_is_right(case, x):
     ("allreduce", "L", 72, 30_001, [6, 12], 2),
     ("allreduce", "B", 384, 131_072, None, 1),
     ("allreduce", "B", 1000, 64_007, None, 1),  # programs of 1,000 leaves: over 48 KB of shared memory
+    # Row-aligned tiles holding the ends of several segments (one tree
+    # shape, ranks per lane): 2 to 8 segments per tile.
+    ("allreduce", "B", 96, 96 * 40 + 3, None, 1),
+    ("allreduce", "B", 384, 384 * 100 + 1, None, 1),
+    ("allreduce", "B", 200, 200 * 1000 + 17, None, 1),
+    ("allreduce", "B", 1000, 1000 * 130 + 3, None, 1),
+    ("allreduce", "B_COALESCE", 96, 96 * 333 + 5, None, 1),
 ])
 def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
     sc, _ = buffer_counts(coll, count, P)
@@ -135,6 +142,23 @@ def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
     assert np.array_equal(out[rr].view(np.uint32), expect[rr].view(np.uint32))
 
 
+@pytest.mark.parametrize("P,count,form", [
+    (96, 96 * 40 + 3, 3), (384, 384 * 100 + 1, 3), (1000, 1000 * 130 + 3, 3),
+    (200, 200 * 1000 + 17, 2),  # three tree shapes (10, 82 and 108 segments)
+    (96, 524_288, 3), (384, 524_288, 3), (1000, 1_048_576, 3),
+    (256, 1 << 20, 3),   # power of two: segments on the grid already, one shape
+    (96, 96 * 8, 2),     # 2-vector segments: a 32-vector tile would touch 16
+])
+def test_row_aligned_tiles_are_used(P, count, form):
+    """The exact-order allreduce plans row-aligned tiles (form 3) where every
+    tree has one shape and a tile touches at most 8 segments, and keeps
+    per-segment tiles otherwise (several shapes, or short segments); the
+    cases above that compare bits with the oracle therefore run both."""
+    comm = make_comm(P, "allreduce", "B")
+    got, lanes = comm.tree_form("allreduce", count, bine.FLOAT)
+    assert (got, lanes > 1) == (form, True)
+
+
 @pytest.mark.parametrize("lanes", [1, 2, 4, 8])
 @pytest.mark.parametrize("coll,variant,P,count,dims,ports", [
     ("allreduce", "B", 256, 256 * 64, None, 1),
@@ -144,6 +168,7 @@ def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
     ("allreduce", "L", 64, 50_000, None, 1),
     ("allreduce", "L", 72, 30_000, [6, 12], 2),
     ("allreduce", "B", 64, 64 * 600, [4, 4, 4], 6),
+    ("allreduce", "B", 384, 384 * 100 + 1, None, 1),
     ("reduce_scatter", "VEC_HALVING_CONT_PERMUTE", 64, 1024, None, 1),
     ("reduce", "BINOMIAL_TREE", 64, 20_000, None, 1),
 ])
@@ -412,6 +437,21 @@ def test_allreduce_host_buffers_float_reference_order(split):
     dev = run(comm, "allreduce", x, count)
     send = torch.from_numpy(x).pin_memory()
     recv = torch.zeros_like(send).pin_memory()
+    comm.allreduce_host(send, recv, count, bine.FLOAT)
+    assert np.array_equal(recv.numpy().view(np.uint32), dev.view(np.uint32))
+
+
+@pytest.mark.parametrize("P,count", [(96, 96 * 333 + 7), (1000, 1000 * 262 + 11)])
+def test_allreduce_host_buffers_float_row_aligned_tiles(P, count):
+    """Non-power-of-two P, exact float order through column windows: the
+    row-aligned tiles clipped at window edges return the device call's
+    bits."""
+    x = np.random.default_rng(P + 5).standard_normal((P, count)).astype(np.float32)
+    comm = make_comm(P, "allreduce", "B")
+    dev = run(comm, "allreduce", x, count)
+    send = torch.from_numpy(x).pin_memory()
+    recv = torch.zeros_like(send).pin_memory()
+    comm.set_host_window(1 << 20)
     comm.allreduce_host(send, recv, count, bine.FLOAT)
     assert np.array_equal(recv.numpy().view(np.uint32), dev.view(np.uint32))
 
