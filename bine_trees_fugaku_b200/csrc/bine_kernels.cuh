@@ -495,27 +495,25 @@ struct FlatArgs {
 };
 
 // Evaluates entries [b, b + len) of a program whose additions are
-// `adds` and whose ranks are rk[k * rstep] (1: a row of the shared-memory
-// rank table; nq: a column of the entry-major global table, so that the
-// lanes of an edge tile, which own consecutive segments, read consecutive
-// words), for one 16-byte vector at `base`; loads run kRing entries ahead
+// `adds[k]` and whose ranks are `rk[k]` (a row of the shared-memory rank
+// table), for one 16-byte vector at `base`; loads run kRing entries ahead
 // of the additions.
 template <typename T, bool SMEM, int kRing>
 __device__ __forceinline__ uint4 eval_ranks(const char* __restrict__ base, long long stride, const uint16_t* rk,
-                                            int rstep, const uint8_t* adds, int b, int len, EvalStack<SMEM>& stk) {
+                                            const uint8_t* adds, int b, int len, EvalStack<SMEM>& stk) {
     uint4 top = make_uint4(0, 0, 0, 0);
     int sp = 0;
     uint4 ring[kRing];
 #pragma unroll
     for (int u = 0; u < kRing; u++)
-        if (u < len) ring[u] = ld_stream(base + (long long)rk[(b + u) * rstep] * stride);
+        if (u < len) ring[u] = ld_stream(base + (long long)rk[b + u] * stride);
     for (int k0 = 0; k0 < len; k0 += kRing) {
 #pragma unroll
         for (int u = 0; u < kRing; u++) {
             const int k = k0 + u;
             if (k < len) {
                 const uint4 v = ring[u];
-                if (k + kRing < len) ring[u] = ld_stream(base + (long long)rk[(b + k + kRing) * rstep] * stride);
+                if (k + kRing < len) ring[u] = ld_stream(base + (long long)rk[b + k + kRing] * stride);
                 if (k > 0) stk.set(sp++, top);
                 top = v;
                 for (int a = adds[b + k]; a > 0; a--) top = vadd<T>(stk.get(--sp), top);
@@ -572,7 +570,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_flat(const FlatArgs A) {
             const uint16_t* rk = sranks + slot * A.pitch;
             for (int pi = sasg[nparts + j]; pi < sasg[nparts + j + 1]; pi++) {
                 const int p = sasg[pi];
-                partial[g][p][lane] = eval_ranks<T, SMEM, 4>(A.in + e * (long long)sizeof(T), A.in_stride, rk, 1,
+                partial[g][p][lane] = eval_ranks<T, SMEM, 4>(A.in + e * (long long)sizeof(T), A.in_stride, rk,
                                                              sadds, spart[p], spart[p + 1] - spart[p], stk);
             }
         }
@@ -589,6 +587,46 @@ __global__ void __launch_bounds__(kThreads) k_tree_flat(const FlatArgs A) {
         for (int d = j; d < A.P; d += K)
             st_stream(A.out + (long long)d * A.out_stride + e * (long long)sizeof(T), top);
     }
+}
+
+// Edge form of eval_ranks: the ranks come from the entry-major global
+// table (`rt` at the lane's segment; entry k at rt[k * nq]) and are read
+// one ring ahead of the loads that use them, so that a rank's L2 latency is
+// not added to every leaf's.
+template <typename T, bool SMEM, int kRing>
+__device__ __forceinline__ uint4 eval_edge(const char* __restrict__ base, long long stride,
+                                           const uint16_t* __restrict__ rt, int nq, const uint8_t* adds, int b,
+                                           int len, EvalStack<SMEM>& stk) {
+    uint4 top = make_uint4(0, 0, 0, 0);
+    int sp = 0;
+    uint4 ring[kRing];
+    int rr[kRing];
+#pragma unroll
+    for (int u = 0; u < kRing; u++)
+        if (u < len) rr[u] = __ldg(rt + (long long)(b + u) * nq);
+#pragma unroll
+    for (int u = 0; u < kRing; u++)
+        if (u < len) {
+            ring[u] = ld_stream(base + (long long)rr[u] * stride);
+            if (u + kRing < len) rr[u] = __ldg(rt + (long long)(b + u + kRing) * nq);
+        }
+    for (int k0 = 0; k0 < len; k0 += kRing) {
+#pragma unroll
+        for (int u = 0; u < kRing; u++) {
+            const int k = k0 + u;
+            if (k < len) {
+                const uint4 v = ring[u];
+                if (k + kRing < len) {
+                    ring[u] = ld_stream(base + (long long)rr[u] * stride);
+                    if (k + 2 * kRing < len) rr[u] = __ldg(rt + (long long)(b + k + 2 * kRing) * nq);
+                }
+                if (k > 0) stk.set(sp++, top);
+                top = v;
+                for (int a = adds[b + k]; a > 0; a--) top = vadd<T>(stk.get(--sp), top);
+            }
+        }
+    }
+    return top;
 }
 
 // The edges of the row-aligned form (see above).  Their trees are cut into
@@ -627,9 +665,9 @@ __global__ void __launch_bounds__(kThreads) k_tree_edges(const FlatArgs A, int n
         if (act) ed = A.edges[ei];
         __syncthreads();  // the previous partials are consumed (and the plan staged)
         if (act)
-            partial[w][lane] = eval_ranks<T, SMEM, 4>(A.in + ed.e * (long long)sizeof(T), A.in_stride,
-                                                      A.ranks_t + ed.q + side, A.nq, sadds, spart[w],
-                                                      spart[w + 1] - spart[w], stk);
+            partial[w][lane] = eval_edge<T, SMEM, 8>(A.in + ed.e * (long long)sizeof(T), A.in_stride,
+                                                     A.ranks_t + ed.q + side, A.nq, sadds, spart[w],
+                                                     spart[w + 1] - spart[w], stk);
         __syncthreads();
         if (!act) continue;
         uint4 top = make_uint4(0, 0, 0, 0);
