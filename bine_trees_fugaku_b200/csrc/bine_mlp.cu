@@ -212,6 +212,16 @@ __device__ __forceinline__ void mma_bf16_16816(float* d, const uint32_t* a, cons
 // kernel issues the next layer's round as soon as this layer's mma chain
 // has consumed the fragments, so that the L2 latency of layer l + 1 runs
 // under layer l's epilogue and block barrier.
+//
+// Which columns of a 32-column block feed which k slots of the mma is free,
+// as long as A and B agree: lane (g, t) gives k-step 2j the columns
+// 32j + 8t + {0,1} (slots 2t, 2t+1) and 32j + 8t + {2,3} (slots 2t+8,
+// 2t+9), and k-step 2j+1 the columns 32j + 8t + {4..7}.  Each lane then
+// reads 16 contiguous bytes of its weight row per two k-steps (one
+// fully-used 32-byte sector pair per row and instruction, a quarter of the
+// load instructions of the mma's natural column order) and 16 contiguous
+// bytes of each activation row.  A trailing single k-step (K not a
+// multiple of 32) takes columns 4t + {0,1} and 4t + {2,3} of its 16.
 struct EnsFrag {
     uint32_t b[16][2];
     float b0, b1;
@@ -222,14 +232,22 @@ __device__ __forceinline__ void ens_fetch(EnsFrag& f, int K, const bf16* __restr
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     if (warp * 8 >= N) return;
-    const int ksteps = K / 16;
-    const bf16* wr = W + (size_t)(warp * 8 + g) * K + 2 * t;
+    const int npair = K / 32;
+    const bf16* wr = W + (size_t)(warp * 8 + g) * K;
 #pragma unroll
-    for (int kk = 0; kk < 16; kk++)
-        if (kk < ksteps) {
-            f.b[kk][0] = __ldg((const unsigned int*)(wr + kk * 16));
-            f.b[kk][1] = __ldg((const unsigned int*)(wr + kk * 16 + 8));
+    for (int j = 0; j < 8; j++) {  // unrolled: the fragment indices stay static (registers)
+        if (j < npair) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(wr + 32 * j + 8 * t));
+            f.b[2 * j][0] = v.x;
+            f.b[2 * j][1] = v.y;
+            f.b[2 * j + 1][0] = v.z;
+            f.b[2 * j + 1][1] = v.w;
+        } else if (j == npair && (K % 32)) {
+            const uint2 v = __ldg(reinterpret_cast<const uint2*>(wr + 32 * j + 4 * t));
+            f.b[2 * j][0] = v.x;
+            f.b[2 * j][1] = v.y;
         }
+    }
     const int c = warp * 8 + 2 * t;
     f.b0 = __ldg(bias + c);
     f.b1 = __ldg(bias + c + 1);
@@ -239,18 +257,23 @@ __device__ __forceinline__ void ens_fetch(EnsFrag& f, int K, const bf16* __restr
 __device__ __forceinline__ void ens_mma(float* acc, const bf16* __restrict__ act, int lda, int K, const EnsFrag& f) {
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    const int ksteps = K / 16;
+    const int npair = K / 32;
 #pragma unroll
-    for (int kk = 0; kk < 16; kk++)
-        if (kk < ksteps) {
-            const int k0 = kk * 16;
-            uint32_t a[4];
-            a[0] = *(const uint32_t*)(act + g * lda + k0 + 2 * t);
-            a[1] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 2 * t);
-            a[2] = *(const uint32_t*)(act + g * lda + k0 + 8 + 2 * t);
-            a[3] = *(const uint32_t*)(act + (g + 8) * lda + k0 + 8 + 2 * t);
-            mma_bf16_16816(acc, a, f.b[kk]);
+    for (int j = 0; j < 8; j++) {
+        if (j < npair) {
+            const uint4 r0 = *reinterpret_cast<const uint4*>(act + g * lda + 32 * j + 8 * t);
+            const uint4 r1 = *reinterpret_cast<const uint4*>(act + (g + 8) * lda + 32 * j + 8 * t);
+            const uint32_t a0[4] = {r0.x, r1.x, r0.y, r1.y};
+            const uint32_t a1[4] = {r0.z, r1.z, r0.w, r1.w};
+            mma_bf16_16816(acc, a0, f.b[2 * j]);
+            mma_bf16_16816(acc, a1, f.b[2 * j + 1]);
+        } else if (j == npair && (K % 32)) {
+            const uint2 r0 = *reinterpret_cast<const uint2*>(act + g * lda + 32 * j + 4 * t);
+            const uint2 r1 = *reinterpret_cast<const uint2*>(act + (g + 8) * lda + 32 * j + 4 * t);
+            const uint32_t a[4] = {r0.x, r1.x, r0.y, r1.y};
+            mma_bf16_16816(acc, a, f.b[2 * j]);
         }
+    }
 }
 
 // Bias and GELU into the next activation buffer, or fp32 output.
@@ -273,7 +296,9 @@ __device__ __forceinline__ void ens_epilogue(const float* acc, float b0, float b
 
 __global__ void __launch_bounds__(kEnsThreads) k_mlp_ensemble(EnsArgs a) {
     namespace cg = cooperative_groups;
-    constexpr int kLd = kEnsH + 8;  // padded rows: fragment loads spread over banks
+    // Padded rows (144 words, 16 mod 32): the 16-byte activation loads of a
+    // quarter warp (rows g, g + 1; t = 0..3) fall on all 32 banks once.
+    constexpr int kLd = kEnsH + 32;
     __shared__ __align__(16) bf16 s_act[2][16 * kLd];
     __shared__ __align__(16) float s_out[16 * kEnsMaxOut];
     cg::cluster_group cluster = cg::this_cluster();
