@@ -1,8 +1,8 @@
 """The learned picker against exhaustive search and the fixed rule, on the
-committed measurements (tests/golden/picker_dataset.npz: 18,459 sampled
+committed measurements (tests/golden/picker_dataset.npz: 22,532 sampled
 calls, every valid arm timed on a B200 with the STEPS engine by
 `python bench.py --suite picker`) and the committed weights trained on the
-calls outside its `test` split (3,869 held-out calls, 2,943 of them with a
+calls outside its `test` split (4,683 held-out calls, 3,579 of them with a
 valid arm).
 
 The CPU test evaluates the weights with the float64 reference of the MLP
@@ -24,7 +24,7 @@ DATASET = os.path.join(HERE, "golden", "picker_dataset.npz")
 # The committed dataset: 6,000 calls measured over the first 66 arms (the
 # RING arms unmeasured, hence invalid, for them), 5,790 calls over all 69
 # arms (half of them held out: the `test` split), 1,798 more for training,
-# then 1,500 and 3,371 more over all 69 arms (a fifth of each held out),
+# then 1,500, 3,371 and 4,073 more over all 69 arms (a fifth of each held out),
 # merged and trained with --picker-data ... --picker-n N.
 
 
@@ -42,12 +42,12 @@ def cpu_predict(X):
 
 def check_gain(ev):
     # The stated target is 95 % of pure picks within 5 % of exhaustive
-    # search.  Measured: 94.2 % (the misses concentrate on the integer
+    # search.  Measured: 93.7 % (the misses concentrate on the integer
     # allreduce, whose 15 arms the picker may all choose from; the re-timing
     # noise ceiling is 98.3-100 %).  The model's three best arms, timed
-    # (Picker.tune), meet the target with 98.9 %.  Learned picks are faster
+    # (Picker.tune), meet the target with 98.8 %.  Learned picks are faster
     # than the fixed rule, which lands within 5 % on 57 % of the calls.
-    assert ev["held_out_calls"] >= 2900
+    assert ev["held_out_calls"] >= 3500
     assert ev["pick_within_5pct_of_optimum"] >= 0.93
     assert ev["pick_within_5pct_of_optimum"] >= ev["fixed_rule_within_5pct_of_optimum"] + 0.3
     assert ev["pick_time_over_optimum_geomean"] <= 1.02
@@ -66,11 +66,12 @@ def test_dataset_is_consistent():
         for a in np.nonzero(valid[i])[0]:
             assert pk.statically_valid(pk.ARMS[a], c["coll"], c["P"], c["count"], c["dims"])
     # Held out: half of the 5,790 calls measured over all 69 arms, and a
-    # fifth of each later batch (1,500 and 3,371 calls).
-    old, b1, b2 = te[te < 6000 + 5790], te[(te >= 13588) & (te < 15088)], te[te >= 15088]
-    assert len(set(te.tolist())) == len(te) == len(old) + len(b1) + len(b2)
+    # fifth of each later batch (1,500, 3,371 and 4,073 calls).
+    old = te[te < 6000 + 5790]
+    b1, b2, b3 = te[(te >= 13588) & (te < 15088)], te[(te >= 15088) & (te < 18459)], te[te >= 18459]
+    assert len(set(te.tolist())) == len(te) == len(old) + len(b1) + len(b2) + len(b3)
     assert len(old) == 5790 // 2 and 6000 <= old.min()
-    assert len(b1) == 1500 // 5 and len(b2) == 3371 // 5 and b2.max() < 18459
+    assert (len(b1), len(b2), len(b3)) == (1500 // 5, 3371 // 5, 4073 // 5) and b3.max() < 22532
 
 
 def test_learned_picks_beat_the_fixed_rule_on_held_out_calls():
