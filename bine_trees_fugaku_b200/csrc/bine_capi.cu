@@ -158,13 +158,13 @@ struct DevTrees {
     bool flat = false;
     int64_t* fbody = nullptr;
     uint16_t* franks = nullptr;
-    uint16_t* franks_t = nullptr;
+    uint8_t* feshape = nullptr;  // edges: the tree shape of each segment, in row order
     uint8_t* fadds = nullptr;
     int* fparts = nullptr;
     dev::TreeComb* fcomb = nullptr;
     int* fassign = nullptr;
     dev::FlatEdge* fedges = nullptr;
-    int fpitch = 0, flen = 0, fmax_ns = 0, fnq = 0;
+    int fpitch = 0, flen = 0, fmax_ns = 0, fnq = 0, fnshape = 1;
     std::vector<dev::FlatEdge> h_fedges;
     // Edges (k_tree_edges): their own split plan, cut into
     // dev::kEdgeParts parts, with its entry-major rank table.
@@ -202,7 +202,7 @@ struct DevTrees {
         cudaFree(stiles);
         cudaFree(fbody);
         cudaFree(franks);
-        cudaFree(franks_t);
+        cudaFree(feshape);
         cudaFree(fedges);
         cudaFree(feadds);
         cudaFree(feparts);
@@ -703,141 +703,191 @@ int get_dev_fused(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevFu
 }
 
 // Tables of the row-aligned split form (k_tree_flat), built when every
-// segment with a vector body sends its result to every rank and its split
-// program has the same additions, part offsets and combine program as the
-// others, with every leaf at shift 0 (allreduce).  Segments are indexed in
-// the order of their bodies.  Row tiles are the output row's own groups of
-// `W` elements that hold some body, each with the first body it touches and
-// how many (at most kFlatSegs, or the form is not used).  Edges are the
-// vectors between two adjacent bodies that straddle their segments'
-// boundary (evaluated with their own split plan `se`, when it has one
-// shape too), and the head and tail pieces the edges cover are listed in
-// `covered` (segment, first element in it) for the element kernel to skip.
-// `sassign` is the split plan's per-segment warp assignment.
+// segment with a vector body sends its result to every rank, every leaf of
+// its split program is at shift 0 (allreduce), and its tree has one of at
+// most kFlatShapes shapes: the shape is the split program's additions, part
+// offsets, combine program and warp assignment, and segments of one shape
+// differ only in their ranks.
+//
+// Row-kernel tables (`body`, `ranks`) list the segments by shape, then by
+// the position of their bodies; shape h occupies [base[h], base[h + 1]).
+// Row tiles are the output row's own groups of `W` elements that hold a
+// body of shape h, each with the first such body it touches and how many
+// (at most kFlatSegs, or the form is not used) in `pad & 0xff`, and h in
+// `pad >> 8`; tiles are ordered by column, then shape, so that the shapes
+// sharing a group's columns run side by side.
+//
+// Edges are the vectors between two bodies adjacent in the row that
+// straddle their segments' boundary.  They are evaluated with the edge
+// split plan `se` (dev::kEdgeParts parts), which must have one structure per
+// shape too; their tables (`eranks_t`, entry-major, and `eshape`) index the
+// segments in row order.  The head and tail pieces the edges cover are
+// listed in `covered` (segment, first element in it) for the element kernel
+// to skip.  `sassign` is the split plan's per-segment warp assignment.
 struct FlatTables {
     std::vector<int64_t> body;
-    std::vector<uint16_t> ranks, ranks_t;
-    std::vector<uint8_t> adds;
+    std::vector<uint16_t> ranks;
+    std::vector<uint8_t> adds;  // [shape][len]
     std::vector<int> parts, assign;
     std::vector<dev::TreeComb> comb;
     std::vector<dev::FlatEdge> edges;
     std::vector<dev::TreeTile> tiles;
-    // The edges' split plan (dev::kEdgeParts parts) and rank table.
-    std::vector<uint8_t> eadds;
+    // The edges' split plans (dev::kEdgeParts parts, per shape) and tables.
+    std::vector<uint8_t> eadds, eshape;
     std::vector<int> eparts;
     std::vector<dev::TreeComb> ecomb;
     std::vector<uint16_t> eranks_t;
     int edepth = 0;
     std::set<std::pair<int32_t, int64_t>> covered;
-    int pitch = 0, len = 0, max_ns = 0, nq = 0;
+    int pitch = 0, len = 0, max_ns = 0, nq = 0, nshape = 0;
 };
 
 bool flat_tables(const TreePlan& tp, const SplitTrees& st, const SplitTrees* se, int K, int KP,
                  const std::vector<int>& sassign, const std::vector<int64_t>& body_lo,
                  const std::vector<int64_t>& body_hi, int64_t W, int L, int P, FlatTables* f) {
     if (P > 65536) return false;
-    std::vector<int> order;
+    std::vector<int> order;  // segments with a body, by position
     for (size_t i = 0; i < tp.segs.size(); i++)
         if (body_lo[i] < body_hi[i]) order.push_back((int)i);
     if (order.empty()) return false;
     std::sort(order.begin(), order.end(),
               [&](int a, int b) { return tp.segs[a].off + body_lo[a] < tp.segs[b].off + body_lo[b]; });
-    const int f0 = order[0];
-    const int32_t* p0 = &st.parts[(size_t)f0 * (KP + 1)];
-    const int len = p0[KP] - p0[0];
     const int NA = KP + K + 1;
-    for (int i : order) {
+    const int len = st.parts[(size_t)order[0] * (KP + 1) + KP] - st.parts[(size_t)order[0] * (KP + 1)];
+    // Shapes, in order of first appearance along the row.
+    std::map<std::vector<int32_t>, int> shape_of;
+    std::vector<int> first_of;  // a segment of each shape
+    std::vector<int> shape(order.size());
+    for (size_t q = 0; q < order.size(); q++) {
+        const int i = order[q];
         if (tp.segs[i].rank >= 0) return false;
         const int32_t* po = &st.parts[(size_t)i * (KP + 1)];
-        for (int j = 0; j <= KP; j++)
-            if (po[j] - po[0] != p0[j] - p0[0]) return false;
-        for (int j = 0; j < KP; j++)
-            if (st.comb[(size_t)i * KP + j] != st.comb[(size_t)f0 * KP + j]) return false;
-        for (int j = 0; j < NA; j++)
-            if (sassign[(size_t)i * NA + j] != sassign[(size_t)f0 * NA + j]) return false;
+        if (po[KP] - po[0] != len) return false;
+        std::vector<int32_t> key;
+        key.reserve(len + 2 * KP + NA + 1);
+        for (int j = 0; j <= KP; j++) key.push_back(po[j] - po[0]);
+        for (int j = 0; j < KP; j++) {
+            key.push_back(st.comb[(size_t)i * KP + j].first);
+            key.push_back(st.comb[(size_t)i * KP + j].second);
+        }
+        for (int j = 0; j < NA; j++) key.push_back(sassign[(size_t)i * NA + j]);
         for (int k = 0; k < len; k++) {
             const ProgEntry& e = st.prog[po[0] + k];
-            const ProgEntry& e0 = st.prog[p0[0] + k];
-            if (e.shift != 0 || e.adds != e0.adds || e.adds < 0 || e.adds > 255 || e.rank < 0 || e.rank >= P)
-                return false;
+            if (e.shift != 0 || e.adds < 0 || e.adds > 255 || e.rank < 0 || e.rank >= P) return false;
+            key.push_back(e.adds);
         }
+        auto it = shape_of.find(key);
+        if (it == shape_of.end()) {
+            if ((int)first_of.size() == dev::kFlatShapes) return false;
+            it = shape_of.emplace(key, (int)first_of.size()).first;
+            first_of.push_back(i);
+        }
+        shape[q] = it->second;
     }
+    const int H = (int)first_of.size();
     const size_t nq = order.size();
+    f->nshape = H;
     f->nq = (int)nq;
     f->len = (len + 15) / 16 * 16;
     f->pitch = (len + 7) / 8 * 8;
-    f->adds.assign(f->len, 0);
-    for (int k = 0; k < len; k++) f->adds[k] = (uint8_t)st.prog[p0[0] + k].adds;
-    for (int j = 0; j <= KP; j++) f->parts.push_back(p0[j] - p0[0]);
-    for (int j = 0; j < KP; j++)
-        f->comb.push_back(dev::TreeComb{st.comb[(size_t)f0 * KP + j].first, st.comb[(size_t)f0 * KP + j].second});
-    f->assign.assign(sassign.begin() + (size_t)f0 * NA, sassign.begin() + (size_t)(f0 + 1) * NA);
-    f->ranks.assign(nq * f->pitch, 0);
-    f->ranks_t.assign((size_t)f->pitch * nq, 0);
-    for (size_t q = 0; q < nq; q++) {
-        const int i = order[q];
+    f->adds.assign((size_t)H * f->len, 0);
+    for (int h = 0; h < H; h++) {
+        const int i = first_of[h];
         const int32_t* po = &st.parts[(size_t)i * (KP + 1)];
-        for (int k = 0; k < len; k++) {
-            const uint16_t r = (uint16_t)st.prog[po[0] + k].rank;
-            f->ranks[q * f->pitch + k] = r;
-            f->ranks_t[(size_t)k * nq + q] = r;
-        }
+        for (int k = 0; k < len; k++) f->adds[(size_t)h * f->len + k] = (uint8_t)st.prog[po[0] + k].adds;
+        for (int j = 0; j <= KP; j++) f->parts.push_back(po[j] - po[0]);
+        for (int j = 0; j < KP; j++)
+            f->comb.push_back(dev::TreeComb{st.comb[(size_t)i * KP + j].first, st.comb[(size_t)i * KP + j].second});
+        f->assign.insert(f->assign.end(), sassign.begin() + (size_t)i * NA, sassign.begin() + (size_t)(i + 1) * NA);
+    }
+    // Row-kernel tables: by shape, then position.
+    std::vector<size_t> gq(nq);  // row-order index of each table entry
+    for (size_t q = 0; q < nq; q++) gq[q] = q;
+    std::stable_sort(gq.begin(), gq.end(), [&](size_t a, size_t b) { return shape[a] < shape[b]; });
+    std::vector<size_t> base(H + 1, 0);
+    for (size_t q = 0; q < nq; q++) base[shape[q] + 1]++;
+    for (int h = 0; h < H; h++) base[h + 1] += base[h];
+    f->ranks.assign(nq * f->pitch, 0);
+    for (size_t x = 0; x < nq; x++) {
+        const int i = order[gq[x]];
+        const int32_t* po = &st.parts[(size_t)i * (KP + 1)];
+        for (int k = 0; k < len; k++) f->ranks[x * f->pitch + k] = (uint16_t)st.prog[po[0] + k].rank;
         f->body.push_back(tp.segs[i].off + body_lo[i]);
         f->body.push_back(tp.segs[i].off + body_hi[i]);
     }
     // Edges: one vector between adjacent bodies, cut by the boundary of
-    // their (adjacent) segments; only with an edge split plan of one shape.
+    // their (adjacent) segments; only with edge split plans of one
+    // structure per shape.
     const int NE = dev::kEdgeParts;
     bool edges_ok = se != nullptr;
-    const int32_t* e0 = edges_ok ? &se->parts[(size_t)f0 * (NE + 1)] : nullptr;
     for (size_t q = 0; edges_ok && q < nq; q++) {
-        const int i = order[q];
+        const int i = order[q], i0 = first_of[shape[q]];
         const int32_t* po = &se->parts[(size_t)i * (NE + 1)];
-        for (int j = 0; j <= NE; j++) edges_ok &= po[j] - po[0] == e0[j] - e0[0];
-        for (int j = 0; j < NE; j++) edges_ok &= se->comb[(size_t)i * NE + j] == se->comb[(size_t)f0 * NE + j];
+        const int32_t* p0 = &se->parts[(size_t)i0 * (NE + 1)];
+        for (int j = 0; j <= NE; j++) edges_ok &= po[j] - po[0] == p0[j] - p0[0];
+        for (int j = 0; j < NE; j++) edges_ok &= se->comb[(size_t)i * NE + j] == se->comb[(size_t)i0 * NE + j];
+        edges_ok &= po[NE] - po[0] == len;
         for (int k = 0; edges_ok && k < len; k++)
-            edges_ok &= se->prog[po[0] + k].adds == se->prog[e0[0] + k].adds && se->prog[po[0] + k].shift == 0;
+            edges_ok &= se->prog[po[0] + k].adds == se->prog[p0[0] + k].adds && se->prog[po[0] + k].shift == 0 &&
+                        se->prog[po[0] + k].adds <= 255;
     }
     if (edges_ok) {
-        f->eadds.assign(f->len, 0);
-        for (int k = 0; k < len; k++) f->eadds[k] = (uint8_t)se->prog[e0[0] + k].adds;
-        for (int j = 0; j <= NE; j++) f->eparts.push_back(e0[j] - e0[0]);
-        for (int j = 0; j < NE; j++)
-            f->ecomb.push_back(dev::TreeComb{se->comb[(size_t)f0 * NE + j].first, se->comb[(size_t)f0 * NE + j].second});
+        f->eadds.assign((size_t)H * f->len, 0);
+        for (int h = 0; h < H; h++) {
+            const int32_t* p0 = &se->parts[(size_t)first_of[h] * (NE + 1)];
+            for (int k = 0; k < len; k++) f->eadds[(size_t)h * f->len + k] = (uint8_t)se->prog[p0[0] + k].adds;
+            for (int j = 0; j <= NE; j++) f->eparts.push_back(p0[j] - p0[0]);
+            for (int j = 0; j < NE; j++)
+                f->ecomb.push_back(dev::TreeComb{se->comb[(size_t)first_of[h] * NE + j].first,
+                                                 se->comb[(size_t)first_of[h] * NE + j].second});
+            int cdepth = 1, sp = 0;
+            for (int j = 0; j < NE; j++) {
+                cdepth = std::max(cdepth, ++sp);
+                sp -= f->ecomb[(size_t)h * NE + j].adds;
+            }
+            f->edepth = std::max(f->edepth, cdepth);
+        }
+        f->edepth = std::max(f->edepth, se->max_depth);
         f->eranks_t.assign((size_t)f->pitch * nq, 0);
         for (size_t q = 0; q < nq; q++) {
+            f->eshape.push_back((uint8_t)shape[q]);
             const int32_t* po = &se->parts[(size_t)order[q] * (NE + 1)];
             for (int k = 0; k < len; k++) f->eranks_t[(size_t)k * nq + q] = (uint16_t)se->prog[po[0] + k].rank;
         }
-        int cdepth = 1, sp = 0;
-        for (int j = 0; j < NE; j++) {
-            cdepth = std::max(cdepth, ++sp);
-            sp -= f->ecomb[j].adds;
-        }
-        f->edepth = std::max(se->max_depth, cdepth);
         for (size_t q = 0; q + 1 < nq; q++) {
             const OutSegment& a = tp.segs[order[q]];
             const OutSegment& b = tp.segs[order[q + 1]];
-            const int64_t e = f->body[2 * q + 1];
-            if (a.off + a.n != b.off || f->body[2 * q + 2] != e + L || b.off <= e || b.off >= e + L) continue;
+            const int64_t e = tp.segs[order[q]].off + body_hi[order[q]];
+            if (a.off + a.n != b.off || b.off + body_lo[order[q + 1]] != e + L || b.off <= e || b.off >= e + L) continue;
             f->edges.push_back(dev::FlatEdge{e, (int32_t)q, (int32_t)(b.off - e)});
             f->covered.insert({order[q], body_hi[order[q]]});
             f->covered.insert({order[q + 1], 0});
         }
     }
-    // Row tiles on the row's grid of W elements.
-    const int64_t first = f->body.front() / W * W, last = f->body.back();
-    size_t q = 0;
-    for (int64_t a = first; a < last; a += W) {
-        const int64_t b = a + W;
-        while (q < nq && f->body[2 * q + 1] <= a) q++;
-        size_t r = q;
-        while (r < nq && f->body[2 * r] < b) r++;
-        if (r == q) continue;
-        if (r - q > (size_t)dev::kFlatSegs) return false;
-        f->max_ns = std::max(f->max_ns, (int)(r - q));
-        f->tiles.push_back(dev::TreeTile{(int32_t)q, (int32_t)(r - q), a, W});
+    // Row tiles on the row's grid of W elements, per shape.
+    for (int h = 0; h < H; h++) {
+        const int64_t* bd = f->body.data() + 2 * base[h];
+        const size_t n = base[h + 1] - base[h];
+        const int64_t first = bd[0] / W * W, last = bd[2 * n - 1];
+        size_t q = 0;
+        for (int64_t a = first; a < last; a += W) {
+            const int64_t b = a + W;
+            while (q < n && bd[2 * q + 1] <= a) q++;
+            if (q == n) break;
+            if (bd[2 * q] >= b) {  // no body of this shape here: skip to the next one's group
+                a = bd[2 * q] / W * W - W;
+                continue;
+            }
+            size_t r = q;
+            while (r < n && bd[2 * r] < b) r++;
+            if (r - q > (size_t)dev::kFlatSegs) return false;
+            f->max_ns = std::max(f->max_ns, (int)(r - q));
+            f->tiles.push_back(dev::TreeTile{(int32_t)(base[h] + q), (int32_t)((r - q) | (h << 8)), a, W});
+        }
     }
+    std::stable_sort(f->tiles.begin(), f->tiles.end(), [](const dev::TreeTile& x, const dev::TreeTile& y) {
+        return x.start != y.start ? x.start < y.start : (x.pad >> 8) < (y.pad >> 8);
+    });
     return true;
 }
 
@@ -1048,7 +1098,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
                 cudaError_t g[9];
                 fill(&d->fbody, ft.body, &g[0]);
                 fill(&d->franks, ft.ranks, &g[1]);
-                fill(&d->franks_t, ft.ranks_t, &g[2]);
+                fill(&d->feshape, ft.eshape, &g[2]);
                 fill(&d->fadds, ft.adds, &g[3]);
                 fill(&d->fparts, ft.parts, &g[4]);
                 fill(&d->fcomb, ft.comb, &g[5]);
@@ -1080,6 +1130,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
                 d->flen = ft.len;
                 d->fmax_ns = ft.max_ns;
                 d->fnq = ft.nq;
+                d->fnshape = ft.nshape;
                 d->h_fedges = ft.edges;
                 stiles = std::move(ft.tiles);
             }
@@ -1291,7 +1342,6 @@ FlatLaunch flat_launch(bine_comm_t c, const DevTrees& d, const char* in, long lo
     a.P = c->P;
     a.body = d.fbody;
     a.ranks = d.franks;
-    a.ranks_t = d.franks_t;
     a.pitch = d.fpitch;
     a.nq = d.fnq;
     a.adds = d.fadds;
@@ -1326,7 +1376,8 @@ template <typename T>
 int launch_tree_edges(bine_comm_t c, const DevTrees& d, const char* in, long long ist, char* out, long long ost,
                       int first, int nedges, cudaStream_t s) {
     if (nedges == 0) return BINE_SUCCESS;
-    const size_t adds = (size_t)d.felen, stack = (size_t)std::max(1, d.fedepth) * dev::kThreads * 16;
+    // Dynamic shared memory: every shape's edge additions, then the stacks.
+    const size_t adds = (size_t)d.fnshape * d.felen, stack = (size_t)std::max(1, d.fedepth) * dev::kThreads * 16;
     const bool in_smem = stack <= 64 * 1024 && adds + stack <= 200 * 1024;
     const size_t smem = adds + (in_smem ? stack : 0);
     dev::FlatArgs a{};
@@ -1342,6 +1393,8 @@ int launch_tree_edges(bine_comm_t c, const DevTrees& d, const char* in, long lon
     a.parts = d.feparts;
     a.comb = d.fecomb;
     a.edges = d.fedges + first;
+    a.shape = d.feshape;
+    a.nshape = d.fnshape;
     a.stack_off = (int)(adds / 16);
     auto kern = in_smem ? dev::k_tree_edges<T, true> : dev::k_tree_edges<T, false>;
     unsigned g = 0;

@@ -441,19 +441,22 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
     }
 }
 
-// Row-aligned form of k_tree_split, for calls whose trees all have one
-// shape.  In allreduce every leaf reads its rank's row at the output's own
-// column, and every segment's tree (one segment per block of the
-// reference's vector) has the same additions: segments differ only in the
-// order of their ranks.  The tiles of k_tree_split start at each segment's
+// Row-aligned form of k_tree_split, for calls whose trees have few
+// shapes.  In allreduce every leaf reads its rank's row at the output's own
+// column, and the segments' trees (one segment per block of the
+// reference's vector) share one shape, or a few (at most kFlatShapes):
+// segments of one shape differ only in the order of their ranks.  The tiles of k_tree_split start at each segment's
 // first 16-byte boundary; with non-power-of-two P that is an arbitrary
 // 16-byte offset, so every 512-byte warp access straddles five 128-byte
 // lines, and a segment's last tile is mostly empty.  Here tiles follow the
 // output row's own grid of 32-vector groups instead: `tile.start` is a
 // multiple of the tile width (in elements, from the row start), a tile may
-// hold the ends of several segments (`tile.pad` of them from `tile.seg`, in
-// the order of their bodies), and each lane evaluates its own segment's
-// ranks.
+// hold the ends of several segments of one shape (`tile.pad & 0xff` of them
+// from `tile.seg`, in the order of their bodies; the shape is
+// `tile.pad >> 8`, and the block stages that shape's plan when it changes),
+// and each lane evaluates its own segment's ranks.  Where segments of
+// several shapes meet in one tile's columns, each shape has its own tile
+// there, and lanes whose vector belongs to another shape idle.
 //
 // A vector that straddles two consecutive segments (an "edge": its first
 // `cut` elements end segment q, the rest begin segment q + 1) is evaluated
@@ -464,9 +467,11 @@ __global__ void __launch_bounds__(kThreads) k_tree_split(const char* __restrict_
 //   body[2q], body[2q+1] segment q's vector body [lo, hi), in elements
 //   ranks[q * pitch + k] the rank of entry k of segment q's split program;
 //   ranks_t[k * nq + q] the same, entry-major (edge lanes read consecutive q)
-//   adds[k]             additions after entry k (the same for every segment)
-//   parts, comb, assign the common split plan (as in k_tree_split)
-constexpr int kFlatSegs = 8;  // segments one row tile may touch
+//   adds[h * len + k]   additions after entry k of shape h's programs
+//   parts, comb, assign shape h's split plan (as in k_tree_split), at
+//                       h * (nparts + 1), h * nparts, h * (nparts + K + 1)
+constexpr int kFlatSegs = 8;    // segments one row tile may touch
+constexpr int kFlatShapes = 8;  // tree shapes one call may have
 
 struct FlatEdge {  // the vector at element `e`: elements [e, e + cut) in segment q, the rest in q + 1
     int64_t e;
@@ -489,6 +494,8 @@ struct FlatArgs {
     const TreeComb* comb;
     const int* assign;
     const FlatEdge* edges;
+    const uint8_t* shape;  // edges: the tree shape of each segment (row order)
+    int nshape;
     const TreeTile* tiles;
     int ntiles, nparts;
     int ranks_off, stack_off;  // dynamic shared memory offsets, in 16-byte words
@@ -542,18 +549,22 @@ __global__ void __launch_bounds__(kThreads) k_tree_flat(const FlatArgs A) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = warp % K, g = warp / K;
     const int nparts = A.nparts;
-    // The common plan, once per block.
-    for (int i = threadIdx.x; i < A.len / 16; i += blockDim.x) sdyn[i] = reinterpret_cast<const uint4*>(A.adds)[i];
-    if (threadIdx.x <= nparts) spart[threadIdx.x] = A.parts[threadIdx.x];
-    if (threadIdx.x < nparts) scomb[threadIdx.x] = A.comb[threadIdx.x];
-    if (threadIdx.x < nparts + K + 1) sasg[threadIdx.x] = A.assign[threadIdx.x];
     const int words = A.pitch / 8;  // 16-byte words of one segment's ranks
     const uint4* granks = reinterpret_cast<const uint4*>(A.ranks);
     uint4* sranks4 = reinterpret_cast<uint4*>(sranks);
+    int cur = -1;  // the tree shape whose plan is staged
     for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
         const TreeTile tile = A.tiles[t];
-        const int s0 = tile.seg, ns = tile.pad;
-        __syncthreads();  // the previous tile's partials and ranks are consumed
+        const int s0 = tile.seg, ns = tile.pad & 0xff, shape = tile.pad >> 8;
+        __syncthreads();  // the previous tile's partials, ranks and plan are consumed
+        if (shape != cur) {  // block-uniform: the plan of this tile's tree shape
+            const uint4* ga = reinterpret_cast<const uint4*>(A.adds + (long long)shape * A.len);
+            for (int i = threadIdx.x; i < A.len / 16; i += blockDim.x) sdyn[i] = ga[i];
+            if (threadIdx.x <= nparts) spart[threadIdx.x] = A.parts[shape * (nparts + 1) + threadIdx.x];
+            if (threadIdx.x < nparts) scomb[threadIdx.x] = A.comb[shape * nparts + threadIdx.x];
+            if (threadIdx.x < nparts + K + 1) sasg[threadIdx.x] = A.assign[shape * (nparts + K + 1) + threadIdx.x];
+            cur = shape;
+        }
         for (int i = threadIdx.x; i < ns * words; i += blockDim.x) sranks4[i] = granks[(long long)s0 * words + i];
         if (threadIdx.x < ns) {
             slo[threadIdx.x] = A.body[2 * (s0 + threadIdx.x)];
@@ -630,9 +641,11 @@ __device__ __forceinline__ uint4 eval_edge(const char* __restrict__ base, long l
 }
 
 // The edges of the row-aligned form (see above).  Their trees are cut into
-// kEdgeParts subtrees of their own (the edge split plan: `parts`, `comb`,
-// `adds`, and ranks_t in that plan's entry order), so that an edge's
-// critical path is P / kEdgeParts leaves whatever the row tiles' split.
+// kEdgeParts subtrees of their own (the edge split plan of each shape h:
+// `parts` at h * (kEdgeParts + 1), `comb` at h * kEdgeParts, `adds` at
+// h * len; ranks_t in that plan's entry order, and `shape` giving each
+// segment's shape), so that an edge's critical path is P / kEdgeParts
+// leaves whatever the row tiles' split.
 // Block b owns edges [32 * (b / 2), +32) and segment side b % 2 (0: the
 // segment the edge vector ends, 1: the one it starts); warp w evaluates
 // part w for its lane's edge, the partial sums meet in shared memory, and
@@ -649,31 +662,40 @@ __global__ void __launch_bounds__(kThreads) k_tree_edges(const FlatArgs A, int n
     EvalStack<SMEM> stk;
     stk.init(sdyn + A.stack_off);
     static_assert(kThreads / 32 == kEdgeParts, "one warp per edge part");
-    __shared__ int spart[kEdgeParts + 1];
-    __shared__ TreeComb scomb[kEdgeParts];
+    // The edge plans of every tree shape (a lane's edge may end a segment
+    // of one shape and begin one of another).
+    __shared__ int spart[kFlatShapes][kEdgeParts + 1];
+    __shared__ TreeComb scomb[kFlatShapes][kEdgeParts];
     __shared__ uint4 partial[kEdgeParts][32];
     constexpr int L = 16 / sizeof(T);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < A.len / 16; i += blockDim.x) sdyn[i] = reinterpret_cast<const uint4*>(A.adds)[i];
-    if (threadIdx.x <= kEdgeParts) spart[threadIdx.x] = A.parts[threadIdx.x];
-    if (threadIdx.x < kEdgeParts) scomb[threadIdx.x] = A.comb[threadIdx.x];
+    for (int i = threadIdx.x; i < A.nshape * A.len / 16; i += blockDim.x)
+        sdyn[i] = reinterpret_cast<const uint4*>(A.adds)[i];
+    for (int i = threadIdx.x; i < A.nshape * (kEdgeParts + 1); i += blockDim.x)
+        spart[i / (kEdgeParts + 1)][i % (kEdgeParts + 1)] = A.parts[i];
+    for (int i = threadIdx.x; i < A.nshape * kEdgeParts; i += blockDim.x)
+        scomb[i / kEdgeParts][i % kEdgeParts] = A.comb[i];
     const int ngroups = (nedges + 31) / 32;
     for (int t = blockIdx.x; t < 2 * ngroups; t += gridDim.x) {
         const int side = t & 1, ei = (t >> 1) * 32 + lane;
         const bool act = ei < nedges;
         FlatEdge ed{0, 0, 0};
-        if (act) ed = A.edges[ei];
-        __syncthreads();  // the previous partials are consumed (and the plan staged)
+        int sh = 0;
+        if (act) {
+            ed = A.edges[ei];
+            sh = A.shape[ed.q + side];
+        }
+        __syncthreads();  // the previous partials are consumed (and the plans staged)
         if (act)
             partial[w][lane] = eval_edge<T, SMEM, 8>(A.in + ed.e * (long long)sizeof(T), A.in_stride,
-                                                     A.ranks_t + ed.q + side, A.nq, sadds, spart[w],
-                                                     spart[w + 1] - spart[w], stk);
+                                                     A.ranks_t + ed.q + side, A.nq, sadds + sh * A.len, spart[sh][w],
+                                                     spart[sh][w + 1] - spart[sh][w], stk);
         __syncthreads();
         if (!act) continue;
         uint4 top = make_uint4(0, 0, 0, 0);
         int csp = 0;
         for (int q = 0; q < kEdgeParts; q++) {
-            const TreeComb c = scomb[q];
+            const TreeComb c = scomb[sh][q];
             if (q > 0) stk.set(csp++, top);
             top = partial[c.part][lane];
             for (int a = c.adds; a > 0; a--) top = vadd<T>(stk.get(--csp), top);

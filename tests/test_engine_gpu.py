@@ -131,6 +131,12 @@ def reference_is_right(case, x):
     ("allreduce", "B", 200, 200 * 1000 + 17, None, 1),
     ("allreduce", "B", 1000, 1000 * 130 + 3, None, 1),
     ("allreduce", "B_COALESCE", 96, 96 * 333 + 5, None, 1),
+    # Several tree shapes: row tiles per shape side by side, edges between
+    # segments of different shapes.
+    ("allreduce", "B", 46, 46 * 2000 + 1, None, 1),
+    ("allreduce", "B", 76, 76 * 3000 + 5, None, 1),
+    ("allreduce", "B", 118, 118 * 500 + 3, None, 1),
+    ("allreduce", "B", 70, 70 * 1000 + 9, None, 1),
 ])
 def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
     sc, _ = buffer_counts(coll, count, P)
@@ -144,16 +150,19 @@ def test_float_exact_order_large(engine, coll, variant, P, count, dims, ports):
 
 @pytest.mark.parametrize("P,count,form", [
     (96, 96 * 40 + 3, 3), (384, 384 * 100 + 1, 3), (1000, 1000 * 130 + 3, 3),
-    (200, 200 * 1000 + 17, 2),  # three tree shapes (10, 82 and 108 segments)
+    (200, 200 * 1000 + 17, 3),  # three tree shapes (10, 82 and 108 segments)
+    (76, 76 * 3000 + 5, 3),     # seven shapes
+    (70, 70 * 1000 + 9, 2),     # nine shapes: more than a call may have
     (96, 524_288, 3), (384, 524_288, 3), (1000, 1_048_576, 3),
     (256, 1 << 20, 3),   # power of two: segments on the grid already, one shape
     (96, 96 * 8, 2),     # 2-vector segments: a 32-vector tile would touch 16
 ])
 def test_row_aligned_tiles_are_used(P, count, form):
-    """The exact-order allreduce plans row-aligned tiles (form 3) where every
-    tree has one shape and a tile touches at most 8 segments, and keeps
-    per-segment tiles otherwise (several shapes, or short segments); the
-    cases above that compare bits with the oracle therefore run both."""
+    """The exact-order allreduce plans row-aligned tiles (form 3) where the
+    trees have at most 8 shapes and a tile touches at most 8 segments of
+    one shape, and keeps per-segment tiles otherwise (more shapes, or short
+    segments); the cases above that compare bits with the oracle therefore
+    run both."""
     comm = make_comm(P, "allreduce", "B")
     got, lanes = comm.tree_form("allreduce", count, bine.FLOAT)
     assert (got, lanes > 1) == (form, True)
@@ -441,7 +450,7 @@ def test_allreduce_host_buffers_float_reference_order(split):
     assert np.array_equal(recv.numpy().view(np.uint32), dev.view(np.uint32))
 
 
-@pytest.mark.parametrize("P,count", [(96, 96 * 333 + 7), (1000, 1000 * 262 + 11)])
+@pytest.mark.parametrize("P,count", [(96, 96 * 333 + 7), (1000, 1000 * 262 + 11), (200, 200 * 700 + 3)])
 def test_allreduce_host_buffers_float_row_aligned_tiles(P, count):
     """Non-power-of-two P, exact float order through column windows: the
     row-aligned tiles clipped at window edges return the device call's
