@@ -138,6 +138,7 @@ def lib():
                            sz, ctypes.POINTER(sz), ctypes.POINTER(ctypes.c_int32), sz, ctypes.POINTER(sz)],
         "bine_plan_trees": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz)],
         "bine_debug_tree_form": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(i), ctypes.POINTER(i)],
+        "bine_plan_tree_form": [vp, i, ctypes.c_long, i, i, i64p],
         "bine_link_bytes_host": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(ctypes.c_uint64), sz],
         "bine_mlp_create": [i, i, i, i, ctypes.c_ulonglong, ctypes.POINTER(vp)],
         "bine_mlp_destroy": [vp],
@@ -447,6 +448,16 @@ class Comm:
         check(lib().bine_plan_trees(self._h, COLL_ID[coll], count, root, prog.ctypes.data_as(p64), npg.value,
                                     ctypes.byref(npg), segs.ctypes.data_as(p64), nsg.value, ctypes.byref(nsg)))
         return prog[: npg.value], segs[: nsg.value]
+
+    def plan_tree_form(self, coll, count, datatype, root=0):
+        """Host-only plan of the exact-order float kernels for this call:
+        dict of form (0 element kernel only, 1 one lane per vector, 2 lanes
+        per vector with per-segment tiles, 3 lanes per vector with
+        row-aligned tiles), lanes, shapes, tiles, edges and element pieces."""
+        o = np.zeros(6, np.int64)
+        check(lib().bine_plan_tree_form(self._h, COLL_ID[coll], count, datatype, root,
+                                        o.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return dict(zip(("form", "lanes", "shapes", "tiles", "edges", "pieces"), (int(v) for v in o)))
 
     def tree_form(self, coll, count, datatype, root=0):
         """(form, lanes) of the exact-order float kernel for this call: form

@@ -183,7 +183,9 @@ struct DevTrees {
         std::vector<int> begin[6];
     };
     std::map<long long, Windows> windows;
+    bool dry = false;  // planned on the host only: nothing was uploaded
     ~DevTrees() {
+        if (dry) return;
         for (auto& kv : windows)
             for (auto* t : kv.second.tiles) cudaFree(t);
         cudaFree(rtiles);
@@ -891,7 +893,10 @@ bool flat_tables(const TreePlan& tp, const SplitTrees& st, const SplitTrees* se,
     return true;
 }
 
-int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTrees>* out) {
+// With `dry` the call plans the trees and their tile lists on the host and
+// uploads nothing (no device is needed; the result is not cached and its
+// device pointers stay null): bine_plan_tree_form reports from it.
+int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTrees>* out, bool dry = false) {
     std::shared_ptr<Schedule> s;
     int rc = get_schedule(c, k, &s);
     if (rc) return rc;
@@ -902,6 +907,12 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
         *out = it->second;
         return BINE_SUCCESS;
     }
+    auto put = [&](auto** dptr, const auto& v, cudaError_t* e) {
+        if (dry)
+            *e = cudaSuccess;
+        else
+            fill(dptr, v, e);
+    };
     TreePlan tp;
     std::string err;
     if (!c->planner->trees(k, *s, &tp, &err)) return fail(BINE_ERR_INTERNAL, err);
@@ -918,6 +929,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
         }
     }
     auto d = std::make_shared<DevTrees>();
+    d->dry = dry;
     std::vector<dev::TreeSeg> segs;
     std::vector<dev::TreeEntry> prog;
     for (const ProgEntry& e : tp.prog) prog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
@@ -990,15 +1002,15 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
         ucomb.push_back(dev::TreeComb{0, 0});
     }
     cudaError_t e1, e2, e3, e4, e5, e6, e7, e8;
-    fill(&d->uparts, uparts, &e7);
-    fill(&d->ucomb, ucomb, &e8);
+    put(&d->uparts, uparts, &e7);
+    put(&d->ucomb, ucomb, &e8);
     if (e7 != cudaSuccess || e8 != cudaSuccess) return fail(BINE_ERR_CUDA, "uploading the reduction trees failed");
-    fill(&d->segs, segs, &e1);
-    fill(&d->prog, prog, &e2);
-    fill(&d->tiles, tiles, &e3);
-    fill(&d->rtiles, rtiles, &e4);
-    fill(&d->htiles, htiles, &e5);
-    fill(&d->atiles, atiles, &e6);
+    put(&d->segs, segs, &e1);
+    put(&d->prog, prog, &e2);
+    put(&d->tiles, tiles, &e3);
+    put(&d->rtiles, rtiles, &e4);
+    put(&d->htiles, htiles, &e5);
+    put(&d->atiles, atiles, &e6);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess || e5 != cudaSuccess ||
         e6 != cudaSuccess)
         return fail(BINE_ERR_CUDA, "uploading the reduction trees failed");
@@ -1096,19 +1108,19 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
             if (flat_tables(tp, st, have_se ? &se : nullptr, K, KP, sassign, body_lo, body_hi,
                             (int64_t)(dev::kThreads / K) * L, (int)L, c->P, &ft)) {
                 cudaError_t g[9];
-                fill(&d->fbody, ft.body, &g[0]);
-                fill(&d->franks, ft.ranks, &g[1]);
-                fill(&d->feshape, ft.eshape, &g[2]);
-                fill(&d->fadds, ft.adds, &g[3]);
-                fill(&d->fparts, ft.parts, &g[4]);
-                fill(&d->fcomb, ft.comb, &g[5]);
-                fill(&d->fassign, ft.assign, &g[6]);
-                fill(&d->fedges, ft.edges, &g[7]);
+                put(&d->fbody, ft.body, &g[0]);
+                put(&d->franks, ft.ranks, &g[1]);
+                put(&d->feshape, ft.eshape, &g[2]);
+                put(&d->fadds, ft.adds, &g[3]);
+                put(&d->fparts, ft.parts, &g[4]);
+                put(&d->fcomb, ft.comb, &g[5]);
+                put(&d->fassign, ft.assign, &g[6]);
+                put(&d->fedges, ft.edges, &g[7]);
                 cudaError_t h[4];
-                fill(&d->feadds, ft.eadds, &h[0]);
-                fill(&d->feparts, ft.eparts, &h[1]);
-                fill(&d->fecomb, ft.ecomb, &h[2]);
-                fill(&d->feranks_t, ft.eranks_t, &h[3]);
+                put(&d->feadds, ft.eadds, &h[0]);
+                put(&d->feparts, ft.eparts, &h[1]);
+                put(&d->fecomb, ft.ecomb, &h[2]);
+                put(&d->feranks_t, ft.eranks_t, &h[3]);
                 for (cudaError_t x : h)
                     if (x != cudaSuccess) return fail(BINE_ERR_CUDA, "uploading the row-aligned reduction trees failed");
                 d->nfedges = (int)ft.edges.size();
@@ -1118,9 +1130,9 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
                 std::vector<dev::TreeTile> keep;
                 for (const dev::TreeTile& t : htiles)
                     if (!ft.covered.count({t.seg, t.start})) keep.push_back(t);
-                cudaFree(d->htiles);
+                if (!dry) cudaFree(d->htiles);
                 d->htiles = nullptr;
-                fill(&d->htiles, keep, &g[8]);
+                put(&d->htiles, keep, &g[8]);
                 for (cudaError_t x : g)
                     if (x != cudaSuccess) return fail(BINE_ERR_CUDA, "uploading the row-aligned reduction trees failed");
                 d->nhtiles = (int)keep.size();
@@ -1137,12 +1149,12 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
             std::vector<dev::TreeEntry> sprog;
             for (const ProgEntry& e : st.prog) sprog.push_back(dev::TreeEntry{e.rank, e.adds, e.shift});
             cudaError_t f1, f2, f3, f4, f5, f6;
-            fill(&d->ssegs, ssegs, &f1);
-            fill(&d->sprog, sprog, &f2);
-            fill(&d->sparts, sparts, &f3);
-            fill(&d->scomb, scomb, &f4);
-            fill(&d->stiles, stiles, &f5);
-            fill(&d->sassign, sassign, &f6);
+            put(&d->ssegs, ssegs, &f1);
+            put(&d->sprog, sprog, &f2);
+            put(&d->sparts, sparts, &f3);
+            put(&d->scomb, scomb, &f4);
+            put(&d->stiles, stiles, &f5);
+            put(&d->sassign, sassign, &f6);
             if (f1 != cudaSuccess || f2 != cudaSuccess || f3 != cudaSuccess || f4 != cudaSuccess || f5 != cudaSuccess ||
                 f6 != cudaSuccess)
                 return fail(BINE_ERR_CUDA, "uploading the split reduction trees failed");
@@ -1160,6 +1172,10 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
             d->h_stiles = stiles;
             d->split_k = K;
         }
+    }
+    if (dry) {
+        *out = d;
+        return BINE_SUCCESS;
     }
     trim(c->dev_trees, kMaxCachedDeviceTables);
     c->dev_trees.emplace(key, d);
@@ -2551,20 +2567,33 @@ int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra) {
     return BINE_SUCCESS;
 }
 
-int bine_debug_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
-                         int* form, int* lanes) {
-    if (!comm || !form || !lanes) return fail(BINE_ERR_ARG, "null argument");
+int bine_plan_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                        int64_t out[6]) {
+    if (!comm || !out) return fail(BINE_ERR_ARG, "null argument");
     if (datatype != BINE_FLOAT && datatype != BINE_DOUBLE) return fail(BINE_ERR_ARG, "not a floating-point type");
     if (!is_reduction(coll)) return fail(BINE_ERR_ARG, "not a reduction");
     if (count <= 0) return fail(BINE_ERR_ARG, "count must be positive");
     if (root < 0 || root >= comm->P) return fail(BINE_ERR_ARG, "root out of range");
-    int rc = ensure_device(comm);
-    if (rc) return rc;
     std::shared_ptr<DevTrees> d;
-    rc = get_dev_trees(comm, make_key(comm, coll, count, root), dtype_size(datatype), &d);
+    int rc = get_dev_trees(comm, make_key(comm, coll, count, root), dtype_size(datatype), &d, true);
     if (rc) return rc;
-    *lanes = d->split_k;
-    *form = d->flat ? 3 : (d->split_k > 1 && d->nstiles > 0 ? 2 : (d->ntiles > 0 ? 1 : 0));
+    out[0] = d->flat ? 3 : (d->split_k > 1 && d->nstiles > 0 ? 2 : (d->ntiles > 0 ? 1 : 0));
+    out[1] = d->split_k;
+    out[2] = d->flat ? d->fnshape : 0;
+    out[3] = d->split_k > 1 ? d->nstiles : d->ntiles;
+    out[4] = d->flat ? d->nfedges : 0;
+    out[5] = (int64_t)d->nhtiles + d->nrtiles;
+    return BINE_SUCCESS;
+}
+
+int bine_debug_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                         int* form, int* lanes) {
+    if (!form || !lanes) return fail(BINE_ERR_ARG, "null argument");
+    int64_t o[6];
+    int rc = bine_plan_tree_form(comm, coll, count, datatype, root, o);
+    if (rc) return rc;
+    *form = (int)o[0];
+    *lanes = (int)o[1];
     return BINE_SUCCESS;
 }
 

@@ -276,12 +276,20 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms);
  * faults or hangs. */
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
 
-/* Which kernel evaluates the vector bodies of an exact-order float
- * reduction on a 16-byte-aligned layout (FUSED engine): *form is 0 (element
- * kernel only), 1 (one lane per vector), 2 (K lanes per vector, tiles per
- * segment) or 3 (K lanes per vector, tiles on the row's own grid, for
- * trees of one shape); *lanes is K.  Plans the call without running it.
- * No reference counterpart: introspection for tests. */
+/* How the FUSED engine evaluates an exact-order float reduction on a
+ * 16-byte-aligned layout, planned on the host only (no device needed;
+ * nothing is uploaded or cached):
+ *   out[0] form: 0 element kernel only, 1 one lane per vector, 2 K lanes per
+ *          vector with tiles per segment, 3 K lanes per vector with tiles on
+ *          the row's own grid (trees of at most 8 shapes);
+ *   out[1] K, the lanes per vector;   out[2] tree shapes (form 3, else 0);
+ *   out[3] vector tiles;   out[4] edge vectors evaluated whole (form 3);
+ *   out[5] element pieces left to the element kernels.
+ * No reference counterpart: introspection of this engine's planner. */
+int bine_plan_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                        int64_t out[6]);
+
+/* out[0] and out[1] of bine_plan_tree_form. */
 int bine_debug_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
                          int *form, int *lanes);
 
