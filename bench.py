@@ -1313,7 +1313,7 @@ def main():
     ap.add_argument("--picker-n", type=int, default=1500)
     ap.add_argument("--picker-seed", type=int, default=11)
     ap.add_argument("--picker-budget", type=float, default=900.0, help="seconds of measurement at most")
-    ap.add_argument("--picker-steps", type=int, default=8000)
+    ap.add_argument("--picker-steps", type=int, default=16000)
     ap.add_argument("--picker-ensemble", type=int, default=5, help="models trained with different seeds, averaged")
     ap.add_argument("--picker-data", default=None,
                     help="measured picker_dataset.npz files to train on (comma-separated; --picker-n 0 to measure none)")

@@ -42,7 +42,7 @@ def cpu_predict(X):
 
 def check_gain(ev):
     # The stated target is 95 % of pure picks within 5 % of exhaustive
-    # search.  Measured: 93.7 % (the misses concentrate on the integer
+    # search.  Measured: 94.2 % (the misses concentrate on the integer
     # allreduce, whose 15 arms the picker may all choose from; the re-timing
     # noise ceiling is 98.3-100 %).  The model's three best arms, timed
     # (Picker.tune), meet the target with 98.8 %.  Learned picks are faster
