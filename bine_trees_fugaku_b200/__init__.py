@@ -139,6 +139,7 @@ def lib():
         "bine_plan_trees": [vp, i, ctypes.c_long, i, i64p, sz, ctypes.POINTER(sz), i64p, sz, ctypes.POINTER(sz)],
         "bine_debug_tree_form": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(i), ctypes.POINTER(i)],
         "bine_plan_tree_form": [vp, i, ctypes.c_long, i, i, i64p],
+        "bine_plan_tree_cover": [vp, i, ctypes.c_long, i, i, i64p, sz, ctypes.POINTER(sz)],
         "bine_link_bytes_host": [vp, i, ctypes.c_long, i, i, ctypes.POINTER(ctypes.c_uint64), sz],
         "bine_mlp_create": [i, i, i, i, ctypes.c_ulonglong, ctypes.POINTER(vp)],
         "bine_mlp_destroy": [vp],
@@ -458,6 +459,18 @@ class Comm:
         check(lib().bine_plan_tree_form(self._h, COLL_ID[coll], count, datatype, root,
                                         o.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
         return dict(zip(("form", "lanes", "shapes", "tiles", "edges", "pieces"), (int(v) for v in o)))
+
+    def plan_tree_cover(self, coll, count, datatype, root=0):
+        """Host-only: the output runs each exact-order kernel of the plan
+        writes, as an array of (first element, elements, kind) rows (kind 1
+        vector tile, 2 edge vector, 3 element piece)."""
+        n = ctypes.c_size_t(0)
+        check(lib().bine_plan_tree_cover(self._h, COLL_ID[coll], count, datatype, root, None, 0, ctypes.byref(n)))
+        runs = np.zeros((max(1, n.value), 3), np.int64)
+        check(lib().bine_plan_tree_cover(self._h, COLL_ID[coll], count, datatype, root,
+                                         runs.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n.value,
+                                         ctypes.byref(n)))
+        return runs[: n.value]
 
     def tree_form(self, coll, count, datatype, root=0):
         """(form, lanes) of the exact-order float kernel for this call: form

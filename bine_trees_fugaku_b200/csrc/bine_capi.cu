@@ -166,6 +166,7 @@ struct DevTrees {
     dev::FlatEdge* fedges = nullptr;
     int fpitch = 0, flen = 0, fmax_ns = 0, fnq = 0, fnshape = 1;
     std::vector<dev::FlatEdge> h_fedges;
+    std::vector<int64_t> h_fbody;  // host copy of fbody (bine_plan_tree_cover)
     // Edges (k_tree_edges): their own split plan, cut into
     // dev::kEdgeParts parts, with its entry-major rank table.
     uint8_t* feadds = nullptr;
@@ -1144,6 +1145,7 @@ int get_dev_trees(bine_comm_t c, const PlanKey& k, int es, std::shared_ptr<DevTr
                 d->fnq = ft.nq;
                 d->fnshape = ft.nshape;
                 d->h_fedges = ft.edges;
+                d->h_fbody = ft.body;
                 stiles = std::move(ft.tiles);
             }
             std::vector<dev::TreeEntry> sprog;
@@ -2564,6 +2566,45 @@ int bine_comm_set_step_timeout(bine_comm_t comm, unsigned timeout_ms) {
 int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra) {
     if (!comm) return fail(BINE_ERR_ARG, "null communicator");
     comm->barrier_extra = extra;
+    return BINE_SUCCESS;
+}
+
+int bine_plan_tree_cover(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                         int64_t* runs, size_t cap, size_t* n) {
+    if (!comm || !n) return fail(BINE_ERR_ARG, "null argument");
+    if (datatype != BINE_FLOAT && datatype != BINE_DOUBLE) return fail(BINE_ERR_ARG, "not a floating-point type");
+    if (!is_reduction(coll)) return fail(BINE_ERR_ARG, "not a reduction");
+    if (count <= 0) return fail(BINE_ERR_ARG, "count must be positive");
+    if (root < 0 || root >= comm->P) return fail(BINE_ERR_ARG, "root out of range");
+    std::shared_ptr<DevTrees> d;
+    const int es = dtype_size(datatype);
+    int rc = get_dev_trees(comm, make_key(comm, coll, count, root), es, &d, true);
+    if (rc) return rc;
+    const int64_t L = 16 / es;
+    std::vector<int64_t> v;  // (first element, elements, kind) triples
+    auto emit = [&](int64_t a, int64_t len, int64_t kind) {
+        v.push_back(a);
+        v.push_back(len);
+        v.push_back(kind);
+    };
+    if (d->flat) {
+        // Row tiles: every lane vector that some slot of the tile's shape owns,
+        // as the kernel finds it.
+        for (const dev::TreeTile& t : d->h_stiles) {
+            const int ns = t.pad & 0xff;
+            for (int64_t e = t.start; e < t.start + t.n; e += L)
+                for (int q = 0; q < ns; q++)
+                    if (e >= d->h_fbody[2 * (t.seg + q)] && e < d->h_fbody[2 * (t.seg + q) + 1]) emit(e, L, 1);
+        }
+        for (const dev::FlatEdge& ed : d->h_fedges) emit(ed.e, L, 2);
+    } else {
+        const std::vector<dev::TreeTile>& vt = d->split_k > 1 ? d->h_stiles : d->h_tiles;
+        for (const dev::TreeTile& t : vt) emit(d->h_seg_off[t.seg] + t.start, t.n, 1);
+    }
+    for (const std::vector<dev::TreeTile>* lst : {&d->h_htiles, &d->h_rtiles})
+        for (const dev::TreeTile& t : *lst) emit(d->h_seg_off[t.seg] + t.start, t.n, 3);
+    *n = v.size() / 3;
+    if (runs && cap >= *n) std::copy(v.begin(), v.end(), runs);
     return BINE_SUCCESS;
 }
 

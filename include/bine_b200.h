@@ -289,6 +289,15 @@ int bine_debug_set_barrier_extra(bine_comm_t comm, unsigned extra);
 int bine_plan_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
                         int64_t out[6]);
 
+/* The output elements each kernel of that plan writes (one output row; all
+ * ranks' rows alike): `n` runs of (first element, elements, kind), kind 1 a
+ * vector tile (a lane vector of a row-aligned tile, or a whole tile of the
+ * other forms), 2 an edge vector, 3 an element piece.  Host only; with
+ * `runs` null or `cap` below the count only `*n` is set.  No reference
+ * counterpart: introspection of this engine's planner. */
+int bine_plan_tree_cover(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
+                         int64_t *runs, size_t cap, size_t *n);
+
 /* out[0] and out[1] of bine_plan_tree_form. */
 int bine_debug_tree_form(bine_comm_t comm, bine_coll_t coll, long count, bine_datatype_t datatype, int root,
                          int *form, int *lanes);

@@ -93,3 +93,32 @@ def test_plan_rejects_integer_types_and_non_reductions():
             c.plan_tree_form("allgather", 1024, bine.FLOAT)
     finally:
         c.close()
+
+
+def coverage(P, count, variant="B"):
+    c = bine.Comm(P)
+    c.set_algo("allreduce", variant)
+    try:
+        runs = c.plan_tree_cover("allreduce", count, bine.FLOAT)
+    finally:
+        c.close()
+    hits = np.zeros(count + 1, np.int64)
+    np.add.at(hits, runs[:, 0], 1)
+    np.add.at(hits, runs[:, 0] + runs[:, 1], -1)
+    return np.cumsum(hits)[:count], runs
+
+
+@pytest.mark.parametrize("P,count", [
+    (96, 524_288), (96, 96 * 40 + 3), (384, 384 * 100 + 1), (1000, 1000 * 130 + 3), (1000, 1_048_577),
+    (200, 200 * 1000 + 17), (76, 76 * 3000 + 5), (46, 46 * 2000 + 1), (70, 70 * 1000 + 9), (96, 96 * 8),
+    (256, 1 << 16), (24, 24 * 1000 + 3),
+])
+def test_every_output_element_is_written_exactly_once(P, count):
+    """The runs the kernels of the plan write (row-tile lane vectors as the
+    kernel finds their segment, edge vectors, element pieces; or the tiles
+    of the per-segment forms) cover the output row once each, with no
+    element written twice: the condition for every kernel to run beside the
+    others without a race, and for no element to be left unwritten."""
+    cover, runs = coverage(P, count)
+    assert cover.min() == 1 and cover.max() == 1
+    assert np.all(runs[:, 1] > 0)
